@@ -1,0 +1,633 @@
+/*
+ * htoracle.c -- CPU restatement of hypertrace's per-pixel path-tracing hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the oracle the CUDA path is checked against; it is
+ * never linked into, called by, or used as a fallback for the product. Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * Parity is pinned two ways (tests/test_oracle_pin.py):
+ *   - against oracle/_ref, the reference's own kernel sources compiled as host C++
+ *     (bit-exact RNG state and radiance for the same scene bytes and seeds);
+ *   - against the committed fixtures in tests/golden/ generated from oracle/_ref.
+ *
+ * Built twice: REAL=float (the f32 path the GPU mirrors) and -DHT_REAL_DOUBLE (the FP64
+ * accuracy oracle, like the reference's DOUBLE_PRECISION build,
+ * kernel/CMakeLists.txt:90-96). Colors stay float in both, as in the reference
+ * (kernel/ocl/algebra/color.hh:6-7).
+ *
+ * Every arithmetic expression keeps the reference's evaluation order and its rounding
+ * points (compile with -ffp-contract=off); each function cites the file:line it restates
+ * (paths relative to the reference project).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string.h>
+#include <stdlib.h>
+#include <pthread.h>
+
+#ifdef HT_REAL_DOUBLE
+typedef double R;
+#define EPS 1e-12
+#define PI_R 3.141592653589793238462643383279502884
+#define RSQRT(x) sqrt(x)
+#define RLOG(x) log(x)
+#define RCOS(x) cos(x)
+#define RSIN(x) sin(x)
+#define RFABS(x) fabs(x)
+#define HTO(name) hto64_##name
+#else
+typedef float R;
+#define EPS 1e-6f
+#define PI_R 3.141592653589793238462643383279502884f
+#define RSQRT(x) sqrtf(x)
+#define RLOG(x) logf(x)
+#define RCOS(x) cosf(x)
+#define RSIN(x) sinf(x)
+#define RFABS(x) fabsf(x)
+#define HTO(name) hto32_##name
+#endif
+
+typedef struct { R x, y; } comp;
+typedef struct { R x, y, z, w; } quat;   /* x = real part; (y, z, w) = i, j, k */
+typedef struct { R x, y, z; } vec3;
+typedef struct { float x, y, z; } col3;
+typedef struct { comp a, b, c, d; } moebius;   /* (a p + b)(c p + d)^-1 */
+typedef struct { vec3 shift; quat rot; } hom3;  /* Chain<Shift3, Rotation3> */
+
+/* Flags. */
+#define HTO_JITTER_YX 1u  /* first jitter draw -> y (g++ host order of random_uniform2) */
+
+enum { RECIPE_HY = 1, RECIPE_EU = 2 };
+enum { OBJ_STRIDE = 128 };
+
+/* ------------------------------------------------------------------ RNG
+ * kernel/ocl/random.cc:8-14: LCG, u = (real)s / (real)2^32. */
+static inline uint32_t rng_next(uint32_t *s) { *s = 1103515245u * *s + 12345u; return *s; }
+static inline R rng_uniform(uint32_t *s) {
+    return (R)rng_next(s) / (R)4294967296.0;
+}
+
+/* ------------------------------------------------------------------ vectors
+ * dot: kernel/ocl/algebra/vector_math.hpp:8-15 (c = 0; c += a[i]*b[i]). */
+static inline R dot2(R ax, R ay, R bx, R by) { R c = 0; c += ax * bx; c += ay * by; return c; }
+static inline R dot3(vec3 a, vec3 b) { R c = 0; c += a.x * b.x; c += a.y * b.y; c += a.z * b.z; return c; }
+static inline R dot4(quat a, quat b) {
+    R c = 0; c += a.x * b.x; c += a.y * b.y; c += a.z * b.z; c += a.w * b.w; return c;
+}
+static inline vec3 v3(R x, R y, R z) { vec3 r = {x, y, z}; return r; }
+static inline quat q4(R x, R y, R z, R w) { quat r = {x, y, z, w}; return r; }
+/* normalize = a / length(a): vector_math.hpp:29-42 */
+static inline vec3 normalize3(vec3 a) { R l = RSQRT(dot3(a, a)); return v3(a.x / l, a.y / l, a.z / l); }
+static inline quat normalize4(quat a) { R l = RSQRT(dot4(a, a)); return q4(a.x / l, a.y / l, a.z / l, a.w / l); }
+static inline vec3 cross3(vec3 a, vec3 b) {  /* vector_math.hpp:16-23 */
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+/* ------------------------------------------------------------------ quaternions
+ * kernel/ocl/algebra/quaternion.cc:4-56 */
+static inline quat q_conj(quat a) { return q4(a.x, -a.y, -a.z, -a.w); }
+static inline quat q_mul(quat a, quat b) {
+    return q4(
+        a.x * b.x - a.y * b.y - a.z * b.z - a.w * b.w,
+        a.x * b.y + a.y * b.x + a.z * b.w - a.w * b.z,
+        a.x * b.z + a.z * b.x - a.y * b.w + a.w * b.y,
+        a.x * b.w + a.w * b.x + a.y * b.z - a.z * b.y);
+}
+static inline quat cq_mul(comp a, quat b) {
+    return q4(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x, a.x * b.z - a.y * b.w, a.x * b.w + a.y * b.z);
+}
+static inline quat q_inverse(quat a) {
+    quat c = q_conj(a); R n = dot4(a, a);
+    return q4(c.x / n, c.y / n, c.z / n, c.w / n);
+}
+static inline quat q_div(quat a, quat b) { return q_mul(a, q_inverse(b)); }
+static inline quat q_add(quat a, quat b) { return q4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+static inline quat q_sub(quat a, quat b) { return q4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+static inline quat q_scale(R k, quat a) { return q4(k * a.x, k * a.y, k * a.z, k * a.w); }
+static inline quat q_divs(quat a, R k) { return q4(a.x / k, a.y / k, a.z / k, a.w / k); }
+static inline quat q_from_c(comp c) { return q4(c.x, c.y, (R)0, (R)0); }  /* q_new(c, C0) */
+
+/* ------------------------------------------------------------------ Moebius
+ * kernel/ocl/transform/moebius.cc:20-56 */
+static inline quat mo_apply_q(moebius m, quat p) {
+    return q_div(q_add(cq_mul(m.a, p), q_from_c(m.b)), q_add(cq_mul(m.c, p), q_from_c(m.d)));
+}
+static inline quat mo_deriv_q(moebius m, quat p, quat v) {
+    quat u = q_add(cq_mul(m.a, p), q_from_c(m.b));
+    quat d = q_add(cq_mul(m.c, p), q_from_c(m.d));
+    R d2 = dot4(d, d);
+    quat g1 = q_div(cq_mul(m.a, v), d);
+    quat cv = cq_mul(m.c, v);
+    quat g21 = q_conj(cv);
+    quat g22 = q_scale(((R)2 * dot4(d, cv)) / d2, q_conj(d));
+    quat g2 = q_mul(u, q_divs(q_sub(g21, g22), d2));
+    return q_add(g1, g2);
+}
+/* mo_inverse = c22_inverse_n (adjugate, det = 1 assumed): matrix_complex.cc:60-65 */
+static inline moebius mo_inverse(moebius m) {
+    moebius r;
+    r.a = m.d;
+    r.b.x = -m.b.x; r.b.y = -m.b.y;
+    r.c.x = -m.c.x; r.c.y = -m.c.y;
+    r.d = m.a;
+    return r;
+}
+
+typedef struct { quat start, dir; } ray_hy;
+typedef struct { vec3 start, dir; } ray_eu;
+
+/* ray_<geo>_map: geometry/ray_map.inl:15-21 (apply_pos, normalize(apply_dir));
+ * mo_apply_dir already normalizes once (moebius.cc:47-49). */
+static inline ray_hy ray_hy_map(ray_hy r, moebius m) {
+    ray_hy o;
+    o.start = mo_apply_q(m, r.start);
+    o.dir = normalize4(normalize4(mo_deriv_q(m, r.start, r.dir)));
+    return o;
+}
+
+/* ------------------------------------------------------------------ Euclidean maps
+ * rotation.cc: rot3_apply_pos = (q (0,p) q*).yzw ; chain.inl:36-73 ; shift.cc:44-59 */
+static inline vec3 rot3_apply(quat q, vec3 p) {
+    quat r = q_mul(q_mul(q, q4((R)0, p.x, p.y, p.z)), q_conj(q));
+    return v3(r.y, r.z, r.w);
+}
+static inline vec3 hom3_apply_pos(hom3 m, vec3 p) {
+    vec3 r = rot3_apply(m.rot, p);
+    return v3(r.x + m.shift.x, r.y + m.shift.y, r.z + m.shift.z);
+}
+static inline vec3 hom3_apply_dir(hom3 m, vec3 d) { return rot3_apply(m.rot, d); }
+static inline hom3 hom3_inverse(hom3 m) {  /* chain.inl:65-73 */
+    hom3 s;
+    s.shift = v3(-m.shift.x, -m.shift.y, -m.shift.z);
+    s.rot = q_conj(m.rot);
+    s.shift = rot3_apply(s.rot, s.shift);  /* rot3_shf3_reorder */
+    return s;
+}
+static inline ray_eu ray_eu_map(ray_eu r, hom3 m) {
+    ray_eu o;
+    o.start = hom3_apply_pos(m, r.start);
+    o.dir = normalize3(hom3_apply_dir(m, r.dir));
+    return o;
+}
+
+/* ------------------------------------------------------------------ hyperbolic geometry
+ * geometry/hyperbolic.cc:20-33 */
+static inline R hy_distance(quat a, quat b) {
+    quat d = q_sub(a, b);
+    R x = (R)1 + dot4(d, d) / ((R)2 * a.z * b.z);
+    return RLOG(x + RSQRT(x * x - (R)1));
+}
+static inline quat hy_dir_at(quat p, quat d, quat h) {
+    R lpxy = RSQRT(dot2(p.x - h.x, p.y - h.y, p.x - h.x, p.y - h.y));
+    R ldxy = RSQRT(dot2(d.x, d.y, d.x, d.y));
+    return q4(h.z / p.z * d.x, h.z / p.z * d.y, d.z - lpxy / p.z * ldxy, (R)0);
+}
+
+/* ------------------------------------------------------------------ shapes
+ * Each returns the hit distance or -1, and on a hit rewrites the ray start/direction
+ * and the local normal. */
+static inline R plane_hy_detect(int repeat, quat *normal, ray_hy *ray) {  /* shape/hy/plane.cc:4-37 */
+    if (repeat) return (R)-1;
+    quat p = ray->start, d = ray->dir;
+    R pd = dot4(p, d);
+    if (RFABS(pd) < EPS) return (R)-1;
+    R s = (R)1 - dot4(p, p);
+    R t = s / ((R)2 * pd);
+    if (t < -EPS) return (R)-1;
+    quat h = q4(p.x + d.x * t, p.y + d.y * t, (R)0, (R)0);
+    R pxy2 = dot2(h.x, h.y, h.x, h.y);
+    if (pxy2 > (R)1) return (R)-1;
+    h.z = RSQRT((R)1 - pxy2);
+    ray->start = h;
+    ray->dir = hy_dir_at(p, d, h);
+    *normal = q4(-h.x, -h.y, -h.z, -h.w);
+    return hy_distance(p, h);
+}
+static inline R horosphere_detect(int repeat, quat *normal, ray_hy *ray) {  /* shape/hy/horosphere.cc:4-34 */
+    quat p = ray->start, d = ray->dir;
+    R dxy = RSQRT(dot2(d.x, d.y, d.x, d.y));
+    if (p.z < dxy) return (R)-1;
+    R dt = RSQRT(p.z * p.z - dxy * dxy);
+    R t = p.z * d.z - dt;
+    R w = EPS * (R)(2 * repeat - 1);
+    if (t < w) {
+        t += (R)2 * dt;
+        if (t < w) return (R)-1;
+    }
+    t /= dxy * dxy;
+    quat h = q4(p.x + d.x * t, p.y + d.y * t, (R)1, (R)0);
+    ray->start = h;
+    ray->dir = hy_dir_at(p, d, h);
+    *normal = q4((R)0, (R)0, (R)-1, (R)0);
+    return hy_distance(p, h);
+}
+static inline R sphere_eu_detect(int repeat, vec3 *normal, ray_eu *ray) {  /* shape/eu/sphere.cc:3-29 */
+    vec3 pos = ray->start, dir = ray->dir;
+    R b = -dot3(dir, pos);
+    vec3 g = v3(pos.x + dir.x * b, pos.y + dir.y * b, pos.z + dir.z * b);
+    R d = (R)1 - dot3(g, g);
+    if (d < (R)0) return (R)-1;
+    d = RSQRT(d);
+    R e = b - d;
+    R w = EPS * (R)(2 * repeat - 1);
+    if (e < w) {
+        e = b + d;
+        if (e < w) return (R)-1;
+    }
+    vec3 h = normalize3(v3(pos.x + dir.x * e, pos.y + dir.y * e, pos.z + dir.z * e));
+    *normal = h;
+    ray->start = h;
+    return e;
+}
+static inline R plane_eu_detect(int repeat, vec3 *normal, ray_eu *ray) {  /* shape/eu/plane.cc:3-21 */
+    if (repeat) return (R)-1;
+    vec3 pos = ray->start, dir = ray->dir;
+    if (pos.z * dir.z > (R)0) return (R)-1;
+    R t = -pos.z / dir.z;
+    ray->start = v3(pos.x + dir.x * t, pos.y + dir.y * t, (R)0);
+    *normal = v3((R)0, (R)0, (R)-1);
+    return t;
+}
+
+/* ------------------------------------------------------------------ materials */
+/* random_hemisphere_cosine: random.cc:37-39,53-59 */
+static inline vec3 hemisphere_cosine(uint32_t *s) {
+    R phi = (R)2 * PI_R * rng_uniform(s);
+    R sqr_cos_theta = rng_uniform(s);
+    R cos_theta = RSQRT(sqr_cos_theta);
+    R sin_theta = RSQRT((R)1 - sqr_cos_theta);
+    return v3(RCOS(phi) * sin_theta, RSIN(phi) * sin_theta, cos_theta);
+}
+/* rot3_look_at_cont / rot3_look_at / rot3_from_axis: transform/rotation.cc */
+static inline quat rot3_look_at_cont(vec3 d) {
+    vec3 z = v3((R)0, (R)0, (R)-1);
+    R c2 = dot3(d, z);
+    R c = RSQRT(((R)1 + c2) / (R)2);
+    R sm = (R)1 / ((R)2 * c);
+    vec3 x = cross3(z, d);
+    return q4(c, sm * x.x, sm * x.y, sm * x.z);
+}
+static inline quat rot3_look_at(vec3 d) {
+    if (d.z < (R)0) return rot3_look_at_cont(d);
+    quat a = rot3_look_at_cont(v3(-d.x, -d.y, -d.z));
+    R half = PI_R / (R)2;
+    R sh = RSIN(half);
+    quat b = q4(RCOS(half), sh * (R)1, sh * (R)0, sh * (R)0);
+    return q_mul(a, b);
+}
+
+typedef struct {
+    col3 diffuse_color; R diffuse_portion;
+    R specular_portion;
+    col3 emission; R luminous_portion;
+    uint32_t shape;
+} material_rec;
+
+/* Mixture interact (material/mixture/impl.inl:16-27 + macros.hh:3-13) with the three
+ * components: Colored<Lambertian> (colored.inl:15-23, lambertian.cc:6-14),
+ * Specular (specular.cc:4-7), Emissive<Absorbing> (emissive.inl:15-23, absorbing.cc:4-6).
+ * Returns false when the path ends. */
+static inline int mixture_interact(const material_rec *m, uint32_t *rng, vec3 normal,
+                                   vec3 *dir, col3 *intensity, col3 *emission) {
+    R alpha = rng_uniform(rng);
+    alpha -= m->diffuse_portion;
+    if (alpha < (R)0) {
+        intensity->x *= m->diffuse_color.x;
+        intensity->y *= m->diffuse_color.y;
+        intensity->z *= m->diffuse_color.z;
+        if (dot3(*dir, normal) > (R)0) normal = v3(-normal.x, -normal.y, -normal.z);
+        vec3 rnd = hemisphere_cosine(rng);
+        quat rot = rot3_look_at(v3(-normal.x, -normal.y, -normal.z));
+        *dir = rot3_apply(rot, rnd);
+        return 1;
+    }
+    alpha -= m->specular_portion;
+    if (alpha < (R)0) {
+        R k = (R)2 * dot3(*dir, normal);
+        *dir = v3(dir->x - k * normal.x, dir->y - k * normal.y, dir->z - k * normal.z);
+        return 1;
+    }
+    alpha -= m->luminous_portion;
+    if (alpha < (R)0) {
+        emission->x += intensity->x * m->emission.x;
+        emission->y += intensity->y * m->emission.y;
+        emission->z += intensity->z * m->emission.z;
+        return 0;
+    }
+    return 0;  /* "unreachable" fall-through of the mixture: the path ends */
+}
+
+/* ------------------------------------------------------------------ scene */
+typedef struct {
+    int recipe;
+    uint32_t n;
+    R fov;
+    col3 background;
+    moebius cam_mo;
+    hom3 cam_hom;
+    moebius *mo;      /* per object map (hyperbolic) */
+    moebius *mo_inv;
+    hom3 *hom;        /* per object map (euclidean) */
+    hom3 *hom_inv;
+    material_rec *mat;
+} scene_t;
+
+static float rd_f(const uint8_t *b, size_t off) { float v; memcpy(&v, b + off, 4); return v; }
+static uint32_t rd_u(const uint8_t *b, size_t off) { uint32_t v; memcpy(&v, b + off, 4); return v; }
+
+static moebius rd_mo(const uint8_t *b) {
+    moebius m;
+    m.a.x = rd_f(b, 0);  m.a.y = rd_f(b, 4);
+    m.b.x = rd_f(b, 8);  m.b.y = rd_f(b, 12);
+    m.c.x = rd_f(b, 16); m.c.y = rd_f(b, 20);
+    m.d.x = rd_f(b, 24); m.d.y = rd_f(b, 28);
+    return m;
+}
+static hom3 rd_hom(const uint8_t *b) {
+    hom3 m;
+    m.shift = v3(rd_f(b, 0), rd_f(b, 4), rd_f(b, 8));
+    m.rot = q4(rd_f(b, 16), rd_f(b, 20), rd_f(b, 24), rd_f(b, 28));
+    return m;
+}
+
+static void scene_free(scene_t *s) {
+    free(s->mo); free(s->mo_inv); free(s->hom); free(s->hom_inv); free(s->mat);
+    memset(s, 0, sizeof(*s));
+}
+
+/* Scene byte ABI: see hypertrace_b200/scene.py (serializer) and include/htcuda.h. */
+static int scene_parse(int recipe, const uint8_t *b, size_t len, int address_width, scene_t *s) {
+    memset(s, 0, sizeof(*s));
+    if (address_width != 32 && address_width != 64) return -4;
+    size_t hdr, objs;
+    if (recipe == RECIPE_HY) { hdr = 96; objs = 128; }
+    else if (recipe == RECIPE_EU) { hdr = 64; objs = 80; }
+    else return -2;
+    if (len < objs) return -1;
+    s->recipe = recipe;
+    s->n = rd_u(b, hdr);
+    if (address_width == 64 && rd_u(b, hdr + 4) != 0) return -1;
+    if ((len - objs) / OBJ_STRIDE < s->n) return -1;
+    s->fov = rd_f(b, 32);
+    size_t bg = recipe == RECIPE_HY ? 64 : 48;
+    s->background.x = rd_f(b, bg); s->background.y = rd_f(b, bg + 4); s->background.z = rd_f(b, bg + 8);
+    uint32_t n = s->n ? s->n : 1;
+    s->mat = (material_rec *)calloc(n, sizeof(material_rec));
+    if (recipe == RECIPE_HY) {
+        s->cam_mo = rd_mo(b);
+        s->mo = (moebius *)calloc(n, sizeof(moebius));
+        s->mo_inv = (moebius *)calloc(n, sizeof(moebius));
+    } else {
+        s->cam_hom = rd_hom(b);
+        s->hom = (hom3 *)calloc(n, sizeof(hom3));
+        s->hom_inv = (hom3 *)calloc(n, sizeof(hom3));
+    }
+    for (uint32_t i = 0; i < s->n; ++i) {
+        const uint8_t *o = b + objs + (size_t)i * OBJ_STRIDE;
+        material_rec *m = &s->mat[i];
+        m->diffuse_color.x = rd_f(o, 32); m->diffuse_color.y = rd_f(o, 36); m->diffuse_color.z = rd_f(o, 40);
+        m->diffuse_portion = rd_f(o, 48);
+        m->specular_portion = rd_f(o, 64);
+        m->emission.x = rd_f(o, 80); m->emission.y = rd_f(o, 84); m->emission.z = rd_f(o, 88);
+        m->luminous_portion = rd_f(o, 96);
+        m->shape = rd_u(o, 112);
+        if (address_width == 64 && rd_u(o, 116) != 0) { scene_free(s); return -1; }
+        if (m->shape > 1) { scene_free(s); return -5; }
+        if (recipe == RECIPE_HY) {
+            s->mo[i] = rd_mo(o);
+            s->mo_inv[i] = mo_inverse(s->mo[i]);
+        } else {
+            s->hom[i] = rd_hom(o);
+            s->hom_inv[i] = hom3_inverse(s->hom[i]);
+        }
+    }
+    return 0;
+}
+
+typedef struct { uint64_t samples, hops, object_tests, hits; } stats_t;
+
+/* <scene>_sample: render/scene.inl:16-44, with the object vector detect of
+ * object/vector.inl:24-62 (nearest hit, ties to the lowest index, hash = index since the
+ * hasher restarts from 0 every hop: hash.cc:11-14, context.cc:11-13) and the mapped
+ * object detect/interact of object/mapped.inl:24-51. */
+static col3 sample_hy(const scene_t *sc, uint32_t hops, uint32_t *rng, R px, R py, R size,
+                      uint32_t flags, stats_t *st) {
+    /* view: view/point/impl.inl:18-25 then view/mapped.inl:20-26 */
+    R u0 = rng_uniform(rng);
+    R u1 = rng_uniform(rng);
+    R jx = (flags & HTO_JITTER_YX) ? u1 : u0;
+    R jy = (flags & HTO_JITTER_YX) ? u0 : u1;
+    R sx = px + size * (jx - (R)0.5f);
+    R sy = py + size * (jy - (R)0.5f);
+    vec3 ld = normalize3(v3(sx, sy, (R)-1 / sc->fov));
+    quat start = q4((R)0, (R)0, (R)1, (R)0);
+    quat dir = q4(ld.x, ld.y, ld.z, (R)0);
+    ray_hy ray;
+    ray.dir = normalize4(mo_deriv_q(sc->cam_mo, start, dir));
+    ray.start = mo_apply_q(sc->cam_mo, start);
+
+    col3 intensity = {1.0f, 1.0f, 1.0f};
+    col3 emission = {0.0f, 0.0f, 0.0f};
+    uint32_t prev_hash = 0xFFFFFFFFu;
+    st->samples += 1;
+    for (uint32_t i = 0; i < hops; ++i) {
+        st->hops += 1;
+        st->object_tests += sc->n;
+        R min_dist = (R)-1;
+        uint32_t min_index = 0;
+        ray_hy min_local = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        quat min_normal = {0, 0, 0, 0};
+        for (uint32_t k = 0; k < sc->n; ++k) {
+            int repeat = (k == prev_hash);
+            ray_hy local = ray_hy_map(ray, sc->mo_inv[k]);
+            quat normal;
+            R dist = sc->mat[k].shape == 0 ? plane_hy_detect(repeat, &normal, &local)
+                                           : horosphere_detect(repeat, &normal, &local);
+            /* the reference maps every candidate back (mapped.inl:34); only the kept one
+             * is observable, so it is mapped back once below */
+            if (dist > -EPS && (min_dist <= -EPS || dist < min_dist)) {
+                min_dist = dist; min_index = k; min_local = local; min_normal = normal;
+            }
+        }
+        if (min_dist > -EPS) {
+            st->hits += 1;
+            ray_hy hit = ray_hy_map(min_local, sc->mo[min_index]);
+            /* interact: mapped.inl:39-51 -> covered.inl:38-56 -> light/hy.cc */
+            ray_hy loc = ray_hy_map(hit, sc->mo_inv[min_index]);
+            vec3 d3 = v3(loc.dir.x, loc.dir.y, loc.dir.z);
+            vec3 n3 = v3(min_normal.x, min_normal.y, min_normal.z);
+            int ret = mixture_interact(&sc->mat[min_index], rng, n3, &d3, &intensity, &emission);
+            loc.dir = q4(d3.x, d3.y, d3.z, (R)0);
+            ray = ray_hy_map(loc, sc->mo[min_index]);
+            if (!ret) break;
+            prev_hash = min_index;
+        } else {
+            /* background/constant.inl:18-21 */
+            emission.x += sc->background.x * intensity.x;
+            emission.y += sc->background.y * intensity.y;
+            emission.z += sc->background.z * intensity.z;
+            break;
+        }
+    }
+    return emission;
+}
+
+static col3 sample_eu(const scene_t *sc, uint32_t hops, uint32_t *rng, R px, R py, R size,
+                      uint32_t flags, stats_t *st) {
+    R u0 = rng_uniform(rng);
+    R u1 = rng_uniform(rng);
+    R jx = (flags & HTO_JITTER_YX) ? u1 : u0;
+    R jy = (flags & HTO_JITTER_YX) ? u0 : u1;
+    R sx = px + size * (jx - (R)0.5f);
+    R sy = py + size * (jy - (R)0.5f);
+    vec3 ld = normalize3(v3(sx, sy, (R)-1 / sc->fov));
+    ray_eu ray;
+    ray.dir = hom3_apply_dir(sc->cam_hom, ld);
+    ray.start = hom3_apply_pos(sc->cam_hom, v3((R)0, (R)0, (R)0));
+
+    col3 intensity = {1.0f, 1.0f, 1.0f};
+    col3 emission = {0.0f, 0.0f, 0.0f};
+    uint32_t prev_hash = 0xFFFFFFFFu;
+    st->samples += 1;
+    for (uint32_t i = 0; i < hops; ++i) {
+        st->hops += 1;
+        st->object_tests += sc->n;
+        R min_dist = (R)-1;
+        uint32_t min_index = 0;
+        ray_eu min_local = {{0, 0, 0}, {0, 0, 0}};
+        vec3 min_normal = {0, 0, 0};
+        for (uint32_t k = 0; k < sc->n; ++k) {
+            int repeat = (k == prev_hash);
+            ray_eu local = ray_eu_map(ray, sc->hom_inv[k]);
+            vec3 normal;
+            R dist = sc->mat[k].shape == 0 ? plane_eu_detect(repeat, &normal, &local)
+                                           : sphere_eu_detect(repeat, &normal, &local);
+            if (dist > -EPS && (min_dist <= -EPS || dist < min_dist)) {
+                min_dist = dist; min_index = k; min_local = local; min_normal = normal;
+            }
+        }
+        if (min_dist > -EPS) {
+            st->hits += 1;
+            ray_eu hit = ray_eu_map(min_local, sc->hom[min_index]);
+            ray_eu loc = ray_eu_map(hit, sc->hom_inv[min_index]);
+            int ret = mixture_interact(&sc->mat[min_index], rng, min_normal, &loc.dir, &intensity, &emission);
+            ray = ray_eu_map(loc, sc->hom[min_index]);
+            if (!ret) break;
+            prev_hash = min_index;
+        } else {
+            emission.x += sc->background.x * intensity.x;
+            emission.y += sc->background.y * intensity.y;
+            emission.z += sc->background.z * intensity.z;
+            break;
+        }
+    }
+    return emission;
+}
+
+/* render: render/render.cl:6-27 for one pixel index. */
+static void render_pixel(const scene_t *sc, uint32_t hops, uint32_t W, uint32_t H, uint32_t px,
+                         float *canvas4, uint32_t *seed, uint32_t flags, stats_t *st) {
+    uint32_t x = px % W, y = px / W;
+    R pxr = ((R)(2u * x + 1u) - (R)W) / (R)H;
+    R pyr = ((R)H - (R)(2u * y + 1u)) / (R)H;
+    R size = (R)2 / (R)H;
+    uint32_t rng = *seed;
+    col3 c = sc->recipe == RECIPE_HY ? sample_hy(sc, hops, &rng, pxr, pyr, size, flags, st)
+                                     : sample_eu(sc, hops, &rng, pxr, pyr, size, flags, st);
+    canvas4[0] += c.x;
+    canvas4[1] += c.y;
+    canvas4[2] += c.z;
+    canvas4[3] += 1.0f;
+    *seed = rng;
+}
+
+typedef struct {
+    const scene_t *sc;
+    uint32_t hops, W, H, passes, flags;
+    const uint32_t *pixels;
+    size_t n;
+    float *canvas;
+    uint32_t *seeds;
+    size_t next;
+    pthread_mutex_t lock;
+} job_t;
+
+typedef struct { job_t *job; stats_t st; } worker_t;
+
+static void *worker_main(void *arg) {
+    worker_t *w = (worker_t *)arg;
+    job_t *j = w->job;
+    const size_t CHUNK = 64;
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        size_t start = j->next;
+        j->next += CHUNK;
+        pthread_mutex_unlock(&j->lock);
+        if (start >= j->n) break;
+        size_t end = start + CHUNK < j->n ? start + CHUNK : j->n;
+        for (size_t i = start; i < end; ++i)
+            for (uint32_t p = 0; p < j->passes; ++p)
+                render_pixel(j->sc, j->hops, j->W, j->H, j->pixels[i], j->canvas + 4 * i,
+                             j->seeds + i, j->flags, &w->st);
+    }
+    return NULL;
+}
+
+/* Renders `passes` passes over the listed pixels; same contract as htref_render.
+ * Returns 0, or a negative error (-1 short/bad scene, -2 unknown recipe, -3 bad hops,
+ * -4 bad address width, -5 bad shape index). */
+int HTO(render)(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, int address_width,
+                uint32_t W, uint32_t H, const uint32_t *pixels, size_t n_pixels, uint32_t passes,
+                float *canvas, uint32_t *seeds, uint32_t flags, int threads, uint64_t *stats) {
+    if (hops == 0) return -3;
+    if (W == 0 || H == 0) return -1;
+    scene_t sc;
+    int rc = scene_parse(recipe, scene, scene_len, address_width, &sc);
+    if (rc != 0) return rc;
+    if (threads < 1) threads = 1;
+    job_t job;
+    job.sc = &sc; job.hops = hops; job.W = W; job.H = H; job.passes = passes; job.flags = flags;
+    job.pixels = pixels; job.n = n_pixels; job.canvas = canvas; job.seeds = seeds; job.next = 0;
+    pthread_mutex_init(&job.lock, NULL);
+    worker_t *ws = (worker_t *)calloc((size_t)threads, sizeof(worker_t));
+    pthread_t *ts = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int t = 0; t < threads; ++t) ws[t].job = &job;
+    for (int t = 1; t < threads; ++t) pthread_create(&ts[t], NULL, worker_main, &ws[t]);
+    worker_main(&ws[0]);
+    for (int t = 1; t < threads; ++t) pthread_join(ts[t], NULL);
+    if (stats) {
+        stats_t s = {0, 0, 0, 0};
+        for (int t = 0; t < threads; ++t) {
+            s.samples += ws[t].st.samples; s.hops += ws[t].st.hops;
+            s.object_tests += ws[t].st.object_tests; s.hits += ws[t].st.hits;
+        }
+        stats[0] = s.samples; stats[1] = s.hops; stats[2] = s.object_tests; stats[3] = s.hits;
+    }
+    free(ws); free(ts);
+    pthread_mutex_destroy(&job.lock);
+    scene_free(&sc);
+    return 0;
+}
+
+/* Post chain: extract (canvas.rs:126-135), gamma (filter/gamma.rs:10-19),
+ * pack (canvas.rs:176-186; OpenCL convert_uchar4 rounds toward zero). */
+void HTO(extract_gamma_pack)(uint32_t n_pixels, uint32_t passes, float gamma, const float *canvas,
+                             float *image, uint8_t *packed) {
+    for (uint32_t i = 0; i < 4u * n_pixels; ++i) {
+        float v = canvas[i] / (float)passes;
+        float m = v > 0.0f ? v : 0.0f;   /* max(x, 0) */
+        float g = powf(m, gamma);
+        if (image) image[i] = g;
+        float c = g < 0.0f ? 0.0f : (g > 1.0f ? 1.0f : g);
+        if (packed) packed[i] = (uint8_t)(255.0f * c);
+    }
+}
+
+int HTO(real_size)(void) { return (int)sizeof(R); }
+
+void HTO(rng_uniforms)(uint32_t seed, uint32_t n, double *out, uint32_t *state_out) {
+    uint32_t s = seed;
+    for (uint32_t i = 0; i < n; ++i) out[i] = (double)rng_uniform(&s);
+    if (state_out) *state_out = s;
+}
