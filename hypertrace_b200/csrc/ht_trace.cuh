@@ -1,0 +1,357 @@
+// ht_trace.cuh -- scene access and the per-hop path logic for the two scene recipes.
+//
+// Device-side restatement of render/scene.inl:16-44 (hop loop), object/vector.inl:24-74
+// (nearest-hit scan), object/mapped.inl:24-51, object/covered.inl:23-56, the shapes in
+// shape/hy/{plane,horosphere}.cc and shape/eu/{plane,sphere}.cc, the mixture material
+// (material/mixture/impl.inl:16-27 with colored.inl, lambertian.cc, specular.cc,
+// emissive.inl, absorbing.cc), the point camera (view/point/impl.inl:18-25,
+// view/mapped.inl:20-26) and the constant background (background/constant.inl:18-21).
+//
+// Scheduling differs from the reference, results do not:
+//  * the object scan keeps only (distance, index) per candidate and recomputes the
+//    winner's local hit afterwards -- the same inputs through the same operations give the
+//    same bits, so this equals keeping every candidate's light/cache copy;
+//  * only the winner is mapped back to world space (the reference maps every candidate
+//    back, mapped.inl:34, but only the kept copy is observable);
+//  * inverse maps are computed once per launch and staged in shared memory.
+#pragma once
+#include "ht_math.cuh"
+
+namespace ht {
+
+constexpr int RECIPE_HY = 1;
+constexpr int RECIPE_EU = 2;
+constexpr float EPSF = 1e-6f;   // EPS for real = float (kernel/ocl/algebra/real.hh:19-25)
+constexpr uint32_t HASH_NEVER = 0xFFFFFFFFu;  // hash_never (kernel/ocl/hash.cc:22-24)
+constexpr uint32_t OBJ_STRIDE = 128;
+constexpr uint32_t FLAG_JITTER_YX = 1u;
+
+// Serialized scene byte offsets (see hypertrace_b200/scene.py for the derivation).
+template <int R> struct Layout;
+template <> struct Layout<RECIPE_HY> {
+    static constexpr uint32_t FOV = 32, BG = 64, COUNT = 96, OBJECTS = 128;
+};
+template <> struct Layout<RECIPE_EU> {
+    static constexpr uint32_t FOV = 32, BG = 48, COUNT = 64, OBJECTS = 80;
+};
+// Object record offsets (Mapped<Covered<Choice, Mixture>, Map>).
+constexpr uint32_t O_DIFFUSE_COLOR = 32, O_DIFFUSE = 48, O_SPECULAR = 64, O_EMISSION = 80,
+                   O_LUMINOUS = 96, O_SHAPE = 112;
+
+struct Material {
+    Col diffuse_color;
+    float diffuse, specular, luminous;
+    Col emission;
+};
+
+HT_D float ldf(const uint8_t *base, uint32_t off) { return __ldg(reinterpret_cast<const float *>(base + off)); }
+HT_D float4 ldf4(const uint8_t *base, uint32_t off) { return __ldg(reinterpret_cast<const float4 *>(base + off)); }
+HT_D uint32_t ldu(const uint8_t *base, uint32_t off) { return __ldg(reinterpret_cast<const uint32_t *>(base + off)); }
+
+HT_D Material load_material(const uint8_t *obj) {
+    Material m;
+    float4 dc = ldf4(obj, O_DIFFUSE_COLOR);
+    m.diffuse_color.x = dc.x; m.diffuse_color.y = dc.y; m.diffuse_color.z = dc.z;
+    m.diffuse = ldf(obj, O_DIFFUSE);
+    m.specular = ldf(obj, O_SPECULAR);
+    float4 em = ldf4(obj, O_EMISSION);
+    m.emission.x = em.x; m.emission.y = em.y; m.emission.z = em.z;
+    m.luminous = ldf(obj, O_LUMINOUS);
+    return m;
+}
+
+HT_D Mo load_mo(const uint8_t *p) {
+    float4 a = ldf4(p, 0), b = ldf4(p, 16);
+    Mo m;
+    m.a.x = a.x; m.a.y = a.y; m.b.x = a.z; m.b.y = a.w;
+    m.c.x = b.x; m.c.y = b.y; m.d.x = b.z; m.d.y = b.w;
+    return m;
+}
+HT_D Hom load_hom(const uint8_t *p) {
+    float4 a = ldf4(p, 0), b = ldf4(p, 16);
+    Hom h;
+    h.shift = v3(a.x, a.y, a.z);
+    h.rot = q4(b.x, b.y, b.z, b.w);
+    return h;
+}
+HT_D Mo mo_from(float4 a, float4 b) {
+    Mo m;
+    m.a.x = a.x; m.a.y = a.y; m.b.x = a.z; m.b.y = a.w;
+    m.c.x = b.x; m.c.y = b.y; m.d.x = b.z; m.d.y = b.w;
+    return m;
+}
+HT_D Hom hom_from(float4 a, float4 b) {
+    Hom h;
+    h.shift = v3(a.x, a.y, a.z);
+    h.rot = q4(b.x, b.y, b.z, b.w);
+    return h;
+}
+
+// Mixture interact: one uniform draw picks the component; returns false when the path ends
+// (Emissive<Absorbing>, or the draw falls past every portion).
+HT_D bool mixture_interact(const Material &m, uint32_t &rng, V3 normal, V3 &dir, Col &intensity,
+                           Col &emission) {
+    float alpha = rng_uniform(rng);
+    alpha -= m.diffuse;
+    if (alpha < 0.0f) {
+        intensity.x *= m.diffuse_color.x;
+        intensity.y *= m.diffuse_color.y;
+        intensity.z *= m.diffuse_color.z;
+        if (dot3(dir, normal) > 0.0f) normal = v3(-normal.x, -normal.y, -normal.z);
+        V3 rnd = hemisphere_cosine(rng);
+        Q4 rot = rot3_look_at(v3(-normal.x, -normal.y, -normal.z));
+        dir = rot3_apply(rot, rnd);
+        return true;
+    }
+    alpha -= m.specular;
+    if (alpha < 0.0f) {
+        float k = 2.0f * dot3(dir, normal);
+        dir = v3(dir.x - k * normal.x, dir.y - k * normal.y, dir.z - k * normal.z);
+        return true;
+    }
+    alpha -= m.luminous;
+    if (alpha < 0.0f) {
+        emission.x += intensity.x * m.emission.x;
+        emission.y += intensity.y * m.emission.y;
+        emission.z += intensity.z * m.emission.z;
+        return false;
+    }
+    return false;
+}
+
+// Staged scene: inverse maps (2 x float4 per object) and shape indices in shared memory.
+struct StagedScene {
+    const float4 *inv;       // shared, 2 per object
+    const uint32_t *shape;   // shared
+    const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials)
+    uint32_t n;
+    float fov;
+    Col background;
+    float4 cam0, cam1;       // camera map (Moebius or Homogenous3) as stored
+};
+
+// -------------------------------------------------------------------------- hyperbolic
+struct HyPath { Q4 p, v; };
+
+// Distance-only plane test (shape/hy/plane.cc:4-37 without the direction update).
+HT_D float plane_hy_dist(Q4 p, Q4 d) {
+    float pd = dot4(p, d);
+    if (fabsf(pd) < EPSF) return -1.0f;
+    float s = 1.0f - dot4(p, p);
+    float t = s / (2.0f * pd);
+    if (t < -EPSF) return -1.0f;
+    float hx = p.x + d.x * t, hy = p.y + d.y * t;
+    float pxy2 = dot2(hx, hy, hx, hy);
+    if (pxy2 > 1.0f) return -1.0f;
+    Q4 h = q4(hx, hy, sqrtf(1.0f - pxy2), 0.0f);
+    return hy_distance(p, h);
+}
+// Distance-only horosphere test (shape/hy/horosphere.cc:4-34).
+HT_D float horosphere_dist(Q4 p, Q4 d, bool repeat) {
+    float dxy = sqrtf(dot2(d.x, d.y, d.x, d.y));
+    if (p.z < dxy) return -1.0f;
+    float dt = sqrtf(p.z * p.z - dxy * dxy);
+    float t = p.z * d.z - dt;
+    float w = repeat ? EPSF : -EPSF;   // EPS * (2*repeat - 1)
+    if (t < w) {
+        t += 2.0f * dt;
+        if (t < w) return -1.0f;
+    }
+    t /= dxy * dxy;
+    Q4 h = q4(p.x + d.x * t, p.y + d.y * t, 1.0f, 0.0f);
+    return hy_distance(p, h);
+}
+// Full tests for the winning object: hit point, transported direction, local normal.
+HT_D void plane_hy_hit(Q4 p, Q4 d, HyPath &hit, Q4 &normal) {
+    float pd = dot4(p, d);
+    float s = 1.0f - dot4(p, p);
+    float t = s / (2.0f * pd);
+    float hx = p.x + d.x * t, hy = p.y + d.y * t;
+    float pxy2 = dot2(hx, hy, hx, hy);
+    Q4 h = q4(hx, hy, sqrtf(1.0f - pxy2), 0.0f);
+    hit.p = h;
+    hit.v = hy_dir_at(p, d, h);
+    normal = q4(-h.x, -h.y, -h.z, -h.w);
+}
+HT_D void horosphere_hit(Q4 p, Q4 d, bool repeat, HyPath &hit, Q4 &normal) {
+    float dxy = sqrtf(dot2(d.x, d.y, d.x, d.y));
+    float dt = sqrtf(p.z * p.z - dxy * dxy);
+    float t = p.z * d.z - dt;
+    float w = repeat ? EPSF : -EPSF;
+    if (t < w) t += 2.0f * dt;
+    t /= dxy * dxy;
+    Q4 h = q4(p.x + d.x * t, p.y + d.y * t, 1.0f, 0.0f);
+    hit.p = h;
+    hit.v = hy_dir_at(p, d, h);
+    normal = q4(0.0f, 0.0f, -1.0f, 0.0f);
+}
+
+// Camera ray: view/point/impl.inl:18-25 (hy_origin = j, hyperbolic.cc:4-6) then the
+// camera Moebius map (view/mapped.inl:20-26).
+HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
+    float u0 = rng_uniform(rng);
+    float u1 = rng_uniform(rng);
+    float jx = (flags & FLAG_JITTER_YX) ? u1 : u0;
+    float jy = (flags & FLAG_JITTER_YX) ? u0 : u1;
+    float sx = px + size * (jx - 0.5f);
+    float sy = py + size * (jy - 0.5f);
+    V3 ld = normalize3(v3(sx, sy, -1.0f / s.fov));
+    HyRay r = view_hy_map(mo_from(s.cam0, s.cam1), q4(0.0f, 0.0f, 1.0f, 0.0f), q4(ld.x, ld.y, ld.z, 0.0f));
+    HyPath o; o.p = r.p; o.v = r.v;
+    return o;
+}
+
+// One hop (one iteration of render/scene.inl:25-41). Returns true while the path goes on.
+// `hit` reports whether the scan found an object (for the hop statistics).
+HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
+                 Col &intensity, Col &emission, bool &hit) {
+    float min_dist = -1.0f;
+    uint32_t kmin = 0;
+    const Q4 p = ray.p, v = ray.v;
+    for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t shape = s.shape[k];
+        const bool repeat = (k == prev_hash);
+        float dist = -1.0f;
+        if (shape == 0) {
+            if (!repeat) {  // a geodesic plane is never hit twice in a row (plane.cc:6-9)
+                HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+                dist = plane_hy_dist(l.p, l.v);
+            }
+        } else {
+            HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+            dist = horosphere_dist(l.p, l.v, repeat);
+        }
+        if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+            min_dist = dist;
+            kmin = k;
+        }
+    }
+    if (!(min_dist > -EPSF)) {
+        hit = false;
+        emission.x += s.background.x * intensity.x;
+        emission.y += s.background.y * intensity.y;
+        emission.z += s.background.z * intensity.z;
+        return false;
+    }
+    hit = true;
+    const Mo inv = mo_from(s.inv[2 * kmin], s.inv[2 * kmin + 1]);
+    const uint8_t *obj = s.objects + (size_t)kmin * OBJ_STRIDE;
+    const Mo fwd = load_mo(obj);
+    const bool repeat = (kmin == prev_hash);
+    HyRay l = ray_hy_map(inv, p, v);
+    HyPath lh;
+    Q4 normal;
+    if (s.shape[kmin] == 0) plane_hy_hit(l.p, l.v, lh, normal);
+    else horosphere_hit(l.p, l.v, repeat, lh, normal);
+    HyRay w = ray_hy_map(fwd, lh.p, lh.v);          // detect: map back (mapped.inl:34)
+    HyRay loc = ray_hy_map(inv, w.p, w.v);          // interact: to local (mapped.inl:46-47)
+    Material m = load_material(obj);
+    V3 dir = v3(loc.v.x, loc.v.y, loc.v.z);          // light_hy_to_local (light/hy.cc:3-8)
+    bool ret = mixture_interact(m, rng, v3(normal.x, normal.y, normal.z), dir, intensity, emission);
+    HyRay out = ray_hy_map(fwd, loc.p, q4(dir.x, dir.y, dir.z, 0.0f));  // mapped.inl:49
+    ray.p = out.p;
+    ray.v = out.v;
+    if (!ret) return false;
+    prev_hash = kmin;   // the hasher state after hash_usize(0, index) is the index
+    return true;
+}
+
+// -------------------------------------------------------------------------- euclidean
+struct EuPath { V3 p, v; };
+
+HT_D float sphere_eu_dist(V3 pos, V3 dir, bool repeat) {   // shape/eu/sphere.cc:3-29
+    float b = -dot3(dir, pos);
+    V3 g = v3(pos.x + dir.x * b, pos.y + dir.y * b, pos.z + dir.z * b);
+    float d = 1.0f - dot3(g, g);
+    if (d < 0.0f) return -1.0f;
+    d = sqrtf(d);
+    float e = b - d;
+    float w = repeat ? EPSF : -EPSF;
+    if (e < w) {
+        e = b + d;
+        if (e < w) return -1.0f;
+    }
+    return e;
+}
+HT_D float plane_eu_dist(V3 pos, V3 dir) {   // shape/eu/plane.cc:3-21 (repeat handled by caller)
+    if (pos.z * dir.z > 0.0f) return -1.0f;
+    return -pos.z / dir.z;
+}
+
+HT_D EuPath camera_eu(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
+    float u0 = rng_uniform(rng);
+    float u1 = rng_uniform(rng);
+    float jx = (flags & FLAG_JITTER_YX) ? u1 : u0;
+    float jy = (flags & FLAG_JITTER_YX) ? u0 : u1;
+    float sx = px + size * (jx - 0.5f);
+    float sy = py + size * (jy - 0.5f);
+    V3 ld = normalize3(v3(sx, sy, -1.0f / s.fov));
+    Hom cam = hom_from(s.cam0, s.cam1);
+    EuPath o;
+    o.v = rot3_apply(cam.rot, ld);                       // hom3_apply_dir: not normalized
+    o.p = hom3_apply_pos(cam, v3(0.0f, 0.0f, 0.0f));
+    return o;
+}
+
+HT_D bool hop_eu(const StagedScene &s, EuPath &ray, uint32_t &rng, uint32_t &prev_hash,
+                 Col &intensity, Col &emission, bool &hit) {
+    float min_dist = -1.0f;
+    uint32_t kmin = 0;
+    const V3 p = ray.p, v = ray.v;
+    for (uint32_t k = 0; k < s.n; ++k) {
+        const uint32_t shape = s.shape[k];
+        const bool repeat = (k == prev_hash);
+        float dist = -1.0f;
+        if (shape == 0) {
+            if (!repeat) {
+                EuRay l = ray_eu_map(hom_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+                dist = plane_eu_dist(l.p, l.v);
+            }
+        } else {
+            EuRay l = ray_eu_map(hom_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+            dist = sphere_eu_dist(l.p, l.v, repeat);
+        }
+        if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+            min_dist = dist;
+            kmin = k;
+        }
+    }
+    if (!(min_dist > -EPSF)) {
+        hit = false;
+        emission.x += s.background.x * intensity.x;
+        emission.y += s.background.y * intensity.y;
+        emission.z += s.background.z * intensity.z;
+        return false;
+    }
+    hit = true;
+    const Hom inv = hom_from(s.inv[2 * kmin], s.inv[2 * kmin + 1]);
+    const uint8_t *obj = s.objects + (size_t)kmin * OBJ_STRIDE;
+    const Hom fwd = load_hom(obj);
+    EuRay l = ray_eu_map(inv, p, v);
+    EuPath lh;
+    V3 normal;
+    lh.v = l.v;
+    if (s.shape[kmin] == 0) {
+        float t = -l.p.z / l.v.z;
+        lh.p = v3(l.p.x + l.v.x * t, l.p.y + l.v.y * t, 0.0f);
+        normal = v3(0.0f, 0.0f, -1.0f);
+    } else {
+        float e = sphere_eu_dist(l.p, l.v, kmin == prev_hash);
+        V3 h = normalize3(v3(l.p.x + l.v.x * e, l.p.y + l.v.y * e, l.p.z + l.v.z * e));
+        lh.p = h;
+        normal = h;
+    }
+    EuRay w = ray_eu_map(fwd, lh.p, lh.v);
+    EuRay loc = ray_eu_map(inv, w.p, w.v);
+    Material m = load_material(obj);
+    V3 dir = loc.v;
+    bool ret = mixture_interact(m, rng, normal, dir, intensity, emission);
+    EuRay out = ray_eu_map(fwd, loc.p, dir);
+    ray.p = out.p;
+    ray.v = out.v;
+    if (!ret) return false;
+    prev_hash = kmin;
+    return true;
+}
+
+}  // namespace ht

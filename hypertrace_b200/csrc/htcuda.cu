@@ -1,0 +1,589 @@
+// htcuda.cu -- kernels and the C ABI of libhtcuda.so (declared in include/htcuda.h).
+//
+// Kernels:
+//   render_plain<R>      one thread per pixel, one pass: the reference's `render` kernel
+//                        (kernel/ocl/render/render.cl:6-27) launched over a (W,H) grid.
+//   render_persistent<R> one launch for P passes: warps pull pixels from a queue with
+//                        warp-aggregated atomics (ballot + popc), each lane runs its pixel's
+//                        P samples in order (the per-pixel RNG stream is sequential), and a
+//                        finished path is regenerated in place, so the object scan runs
+//                        with full warps instead of draining lanes as paths end.
+//   post kernels         extract / gamma / pack (processing/src/canvas.rs:126-135,176-186,
+//                        processing/src/filter/gamma.rs:10-19) and their fused form.
+// Both render kernels stage the scene's inverse object maps and shape indices in shared
+// memory once per block; the object scan reads them as warp-uniform broadcasts.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/htcuda.h"
+#include "ht_trace.cuh"
+
+using namespace ht;
+
+// ============================================================================ errors
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+static int cuda_fail(cudaError_t e, const char *what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return HTC_ERR_CUDA;
+}
+#define HTC_CUDA(call)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Device error word bits.
+constexpr uint32_t ERR_SCENE = 1u;
+constexpr uint32_t ERR_SMEM = 2u;
+
+struct htc_program {
+    int recipe;
+    uint32_t hops;
+    int address_width;
+    uint32_t flags;
+    uint32_t *d_err;     // device error word
+    uint32_t *d_queue;   // [0] next pixel, [1] finished blocks (persistent kernel)
+    int num_sms;
+    int max_smem;
+};
+
+// ============================================================================ staging
+// Loads the scene header and the inverse maps / shape indices of every object into shared
+// memory. Returns false (uniformly across the block) when the scene bytes fail validation.
+template <int R>
+__device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t max_objects,
+                            int address_width, uint32_t *err, StagedScene &s, float4 *s_inv,
+                            uint32_t *s_shape, uint32_t *s_hdr) {
+    using L = Layout<R>;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        uint32_t ok = 1;
+        uint32_t n = 0;
+        if (scene_size < L::OBJECTS) ok = 0;
+        if (ok) {
+            n = ldu(scene, L::COUNT);
+            if (address_width == 64 && ldu(scene, L::COUNT + 4) != 0) ok = 0;
+            if ((scene_size - L::OBJECTS) / OBJ_STRIDE < n) ok = 0;
+            if (n > max_objects) ok = 0;
+        }
+        s_hdr[0] = ok;
+        s_hdr[1] = n;
+    }
+    __syncthreads();
+    const uint32_t n = s_hdr[1];
+    const bool header_ok = s_hdr[0] != 0;
+    __syncthreads();
+    if (!header_ok) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(err, ERR_SCENE);
+        return false;
+    }
+    const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const uint32_t nthreads = blockDim.x * blockDim.y;
+    bool bad = false;
+    for (uint32_t k = tid; k < n; k += nthreads) {
+        const uint8_t *obj = scene + L::OBJECTS + (size_t)k * OBJ_STRIDE;
+        uint32_t shape = ldu(obj, O_SHAPE);
+        if (address_width == 64 && ldu(obj, O_SHAPE + 4) != 0) bad = true;
+        if (shape > 1) bad = true;
+        s_shape[k] = shape;
+        if (R == RECIPE_HY) {
+            Mo inv = mo_inverse(load_mo(obj));
+            s_inv[2 * k] = make_float4(inv.a.x, inv.a.y, inv.b.x, inv.b.y);
+            s_inv[2 * k + 1] = make_float4(inv.c.x, inv.c.y, inv.d.x, inv.d.y);
+        } else {
+            Hom inv = hom3_inverse(load_hom(obj));
+            s_inv[2 * k] = make_float4(inv.shift.x, inv.shift.y, inv.shift.z, 0.0f);
+            s_inv[2 * k + 1] = make_float4(inv.rot.x, inv.rot.y, inv.rot.z, inv.rot.w);
+        }
+    }
+    const int any_bad = __syncthreads_or(bad ? 1 : 0);
+    if (any_bad) {
+        if (tid == 0) atomicOr(err, ERR_SCENE);
+        return false;
+    }
+    s.inv = s_inv;
+    s.shape = s_shape;
+    s.objects = scene + L::OBJECTS;
+    s.n = n;
+    s.fov = ldf(scene, L::FOV);
+    float4 bg = ldf4(scene, L::BG);
+    s.background.x = bg.x; s.background.y = bg.y; s.background.z = bg.z;
+    s.cam0 = ldf4(scene, 0);
+    s.cam1 = ldf4(scene, 16);
+    return true;
+}
+
+template <int R> struct PathOf;
+template <> struct PathOf<RECIPE_HY> { using T = HyPath; };
+template <> struct PathOf<RECIPE_EU> { using T = EuPath; };
+
+template <int R>
+__device__ __forceinline__ typename PathOf<R>::T camera(const StagedScene &s, float px, float py,
+                                                        float size, uint32_t &rng, uint32_t flags) {
+    if constexpr (R == RECIPE_HY) return camera_hy(s, px, py, size, rng, flags);
+    else return camera_eu(s, px, py, size, rng, flags);
+}
+template <int R>
+__device__ __forceinline__ bool hop(const StagedScene &s, typename PathOf<R>::T &ray, uint32_t &rng,
+                                    uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit) {
+    if constexpr (R == RECIPE_HY) return hop_hy(s, ray, rng, prev_hash, intensity, emission, hit);
+    else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit);
+}
+
+// Pixel centre and size (render.cl:12-18).
+__device__ __forceinline__ void pixel_pos(uint32_t x, uint32_t y, uint32_t W, uint32_t H, float &px,
+                                          float &py, float &size) {
+    px = (__uint2float_rn(2u * x + 1u) - __uint2float_rn(W)) / __uint2float_rn(H);
+    py = (__uint2float_rn(H) - __uint2float_rn(2u * y + 1u)) / __uint2float_rn(H);
+    size = 2.0f / __uint2float_rn(H);
+}
+
+__device__ __forceinline__ void flush_stats(uint64_t *stats, uint64_t samples, uint64_t hops,
+                                            uint64_t hits, uint32_t n_objects) {
+    if (!stats) return;
+    for (int off = 16; off > 0; off >>= 1) {
+        samples += __shfl_down_sync(0xffffffffu, samples, off);
+        hops += __shfl_down_sync(0xffffffffu, hops, off);
+        hits += __shfl_down_sync(0xffffffffu, hits, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_SAMPLES], (unsigned long long)samples);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_HOPS], (unsigned long long)hops);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_OBJECT_TESTS], (unsigned long long)(hops * n_objects));
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_HITS], (unsigned long long)hits);
+    }
+}
+
+// ============================================================================ plain
+template <int R>
+__global__ void __launch_bounds__(128) render_plain(
+    const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
+    uint32_t W, uint32_t H, uint32_t hops, uint32_t flags, float4 *__restrict__ canvas,
+    uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t s_hdr[2];
+    float4 *s_inv = smem;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 2 * max_objects);
+    StagedScene s;
+    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_shape, s_hdr)) return;
+
+    // 128 threads = 32 x 4 pixels: each warp covers 32 consecutive pixels of a row.
+    const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const uint32_t y = blockIdx.y * 4 + (threadIdx.x >> 5);
+    const bool inside = x < W && y < H;
+    uint64_t n_samples = 0, n_hops = 0, n_hits = 0;
+    if (inside) {
+        const uint32_t idx = x + W * y;
+        float px, py, size;
+        pixel_pos(x, y, W, H, px, py, size);
+        uint32_t rng = seeds[idx];
+        auto ray = camera<R>(s, px, py, size, rng, flags);
+        Col intensity = {1.0f, 1.0f, 1.0f};
+        Col emission = {0.0f, 0.0f, 0.0f};
+        uint32_t prev_hash = HASH_NEVER;
+        for (uint32_t i = 0; i < hops; ++i) {
+            bool hit;
+            n_hops += 1;
+            bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit);
+            n_hits += hit ? 1 : 0;
+            if (!go) break;
+        }
+        n_samples = 1;
+        float4 c = canvas[idx];
+        c.x += emission.x; c.y += emission.y; c.z += emission.z; c.w += 1.0f;
+        canvas[idx] = c;
+        seeds[idx] = rng;
+    }
+    flush_stats(stats, n_samples, n_hops, n_hits, s.n);
+}
+
+// ============================================================================ persistent
+constexpr uint32_t NO_PIXEL = 0xFFFFFFFFu;
+
+template <int R>
+__global__ void __launch_bounds__(128) render_persistent(
+    const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
+    uint32_t W, uint32_t H, uint32_t hops, uint32_t passes, uint32_t flags,
+    float4 *__restrict__ canvas, uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err,
+    uint32_t *queue) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t s_hdr[2];
+    float4 *s_inv = smem;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 2 * max_objects);
+    StagedScene s;
+    const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_shape, s_hdr);
+
+    const uint32_t total = W * H;
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t n_samples = 0, n_hops = 0, n_hits = 0;
+
+    if (staged) {
+        uint32_t pixel = NO_PIXEL;
+        bool done = false;
+        uint32_t pass = 0, rng = 0, prev_hash = HASH_NEVER, hop_i = 0;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        float px = 0.f, py = 0.f, size = 0.f;
+        typename PathOf<R>::T ray;
+        Col intensity = {1.0f, 1.0f, 1.0f};
+        Col emission = {0.0f, 0.0f, 0.0f};
+        bool in_path = false;
+
+        for (;;) {
+            // Lanes without a pixel take the next ones from the queue: one atomic per warp.
+            const bool need = !done && pixel == NO_PIXEL;
+            const uint32_t mask = __ballot_sync(0xffffffffu, need);
+            if (mask) {
+                uint32_t base = 0;
+                const int leader = __ffs(mask) - 1;
+                if (lane == (uint32_t)leader) base = atomicAdd(&queue[0], (uint32_t)__popc(mask));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (need) {
+                    const uint32_t mine = base + __popc(mask & ((1u << lane) - 1u));
+                    if (mine < total) {
+                        pixel = mine;
+                        const uint32_t x = pixel % W, y = pixel / W;
+                        pixel_pos(x, y, W, H, px, py, size);
+                        rng = seeds[pixel];
+                        acc = canvas[pixel];
+                        pass = 0;
+                        in_path = false;
+                        if (passes == 0) {   // nothing to render: leave the pixel as it is
+                            pixel = NO_PIXEL;
+                        }
+                    } else {
+                        done = true;
+                    }
+                }
+            }
+            if (__all_sync(0xffffffffu, done)) break;
+            if (pixel != NO_PIXEL && !in_path) {
+                ray = camera<R>(s, px, py, size, rng, flags);
+                intensity.x = intensity.y = intensity.z = 1.0f;
+                emission.x = emission.y = emission.z = 0.0f;
+                prev_hash = HASH_NEVER;
+                hop_i = 0;
+                in_path = true;
+            }
+            if (in_path) {
+                bool hit;
+                n_hops += 1;
+                bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit);
+                n_hits += hit ? 1 : 0;
+                hop_i += 1;
+                if (!go || hop_i >= hops) {
+                    acc.x += emission.x; acc.y += emission.y; acc.z += emission.z; acc.w += 1.0f;
+                    n_samples += 1;
+                    in_path = false;
+                    pass += 1;
+                    if (pass >= passes) {
+                        canvas[pixel] = acc;
+                        seeds[pixel] = rng;
+                        pixel = NO_PIXEL;
+                    }
+                }
+            }
+        }
+    }
+    flush_stats(stats, n_samples, n_hops, n_hits, staged ? s.n : 0);
+
+    // The last block to finish rewinds the queue for the next launch.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t finished = atomicAdd(&queue[1], 1u);
+        if (finished == gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ============================================================================ post
+// pow(max(x, 0), gamma) is evaluated in FP64 and rounded once (the host libm's powf is
+// within a fraction of an ulp of that).
+__device__ __forceinline__ float gamma1(float x, float g) {
+    float m = fmaxf(x, 0.0f);
+    return (float)pow((double)m, (double)g);
+}
+__device__ __forceinline__ uint8_t pack1(float x) {
+    float c = fminf(fmaxf(x, 0.0f), 1.0f);
+    return (uint8_t)__float2uint_rz(255.0f * c);
+}
+
+__global__ void k_extract(uint32_t n, float passes, const float4 *__restrict__ canvas, float4 *__restrict__ image) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = canvas[i];
+        image[i] = make_float4(c.x / passes, c.y / passes, c.z / passes, c.w / passes);
+    }
+}
+__global__ void k_gamma(uint32_t n, float g, const float4 *__restrict__ in, float4 *__restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = in[i];
+        out[i] = make_float4(gamma1(c.x, g), gamma1(c.y, g), gamma1(c.z, g), gamma1(c.w, g));
+    }
+}
+__global__ void k_pack(uint32_t n, const float4 *__restrict__ in, uchar4 *__restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = in[i];
+        out[i] = make_uchar4(pack1(c.x), pack1(c.y), pack1(c.z), pack1(c.w));
+    }
+}
+__global__ void k_extract_gamma_pack(uint32_t n, float passes, float g, const float4 *__restrict__ canvas,
+                                     uchar4 *__restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = canvas[i];
+        out[i] = make_uchar4(pack1(gamma1(c.x / passes, g)), pack1(gamma1(c.y / passes, g)),
+                             pack1(gamma1(c.z / passes, g)), pack1(gamma1(c.w / passes, g)));
+    }
+}
+
+// ============================================================================ C ABI
+static int check_program(const htc_program *p) {
+    if (!p) return fail(HTC_ERR_INVALID, "program is NULL");
+    return HTC_OK;
+}
+static size_t smem_bytes(uint32_t max_objects) {
+    return (size_t)max_objects * 32u + (size_t)max_objects * 4u + 16u;
+}
+static uint32_t objects_capacity(int recipe, size_t scene_size) {
+    const size_t hdr = recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
+    if (scene_size < hdr) return 0;
+    size_t n = (scene_size - hdr) / OBJ_STRIDE;
+    return n > 0xFFFFFFu ? 0xFFFFFFu : (uint32_t)n;
+}
+
+template <int R>
+static int set_smem_attr(size_t smem) {
+    HTC_CUDA(cudaFuncSetAttribute(render_plain<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HTC_CUDA(cudaFuncSetAttribute(render_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return HTC_OK;
+}
+
+static int validate_render_args(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                                const float *canvas, const uint32_t *seeds, uint32_t *max_objects, size_t *smem) {
+    int rc = check_program(p);
+    if (rc) return rc;
+    if (W == 0 || H == 0) return fail(HTC_ERR_INVALID, "canvas width and height must be positive");
+    if ((uint64_t)W * (uint64_t)H >= 0xFFFFFFFFull) return fail(HTC_ERR_INVALID, "canvas too large (W*H must fit in 32 bits)");
+    if (!scene || !canvas || !seeds) return fail(HTC_ERR_INVALID, "scene, canvas and seeds must be device pointers");
+    if ((reinterpret_cast<uintptr_t>(scene) & 15u) != 0 || (reinterpret_cast<uintptr_t>(canvas) & 15u) != 0)
+        return fail(HTC_ERR_INVALID, "scene and canvas must be 16-byte aligned");
+    *max_objects = objects_capacity(p->recipe, scene_size);
+    if (scene_size < (p->recipe == HTC_RECIPE_HY ? 128u : 80u))
+        return fail(HTC_ERR_SCENE, "scene buffer is smaller than the scene header");
+    *smem = smem_bytes(*max_objects);
+    if (*smem > (size_t)p->max_smem)
+        return fail(HTC_ERR_UNSUPPORTED, "scene has more objects than shared memory can stage");
+    return HTC_OK;
+}
+
+extern "C" {
+
+const char *htc_last_error(void) { return g_last_error.c_str(); }
+int htc_version(void) { return 10000; }
+
+int htc_device_count(int *count) {
+    if (!count) return fail(HTC_ERR_INVALID, "count is NULL");
+    HTC_CUDA(cudaGetDeviceCount(count));
+    return HTC_OK;
+}
+int htc_set_device(int device) {
+    HTC_CUDA(cudaSetDevice(device));
+    return HTC_OK;
+}
+
+int htc_program_create(int recipe, uint32_t light_hops, int address_width, int double_support,
+                       uint32_t flags, htc_program **out) {
+    if (!out) return fail(HTC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU) return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
+    if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
+    if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
+    if (double_support) return fail(HTC_ERR_UNSUPPORTED, "double_support scenes are not served (f32 transport)");
+    if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    int dev = 0;
+    HTC_CUDA(cudaGetDevice(&dev));
+    htc_program *p = new htc_program();
+    p->recipe = recipe;
+    p->hops = light_hops;
+    p->address_width = address_width;
+    p->flags = flags;
+    cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_err, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_queue, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(p->d_queue, 0, 2 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        if (p->d_err) cudaFree(p->d_err);
+        if (p->d_queue) cudaFree(p->d_queue);
+        delete p;
+        return cuda_fail(e, "htc_program_create");
+    }
+    p->max_smem -= 1024;   // static shared memory of the kernels
+    int rc = recipe == HTC_RECIPE_HY ? set_smem_attr<RECIPE_HY>(p->max_smem) : set_smem_attr<RECIPE_EU>(p->max_smem);
+    if (rc) {
+        cudaFree(p->d_err);
+        cudaFree(p->d_queue);
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return HTC_OK;
+}
+
+void htc_program_destroy(htc_program *p) {
+    if (!p) return;
+    cudaFree(p->d_err);
+    cudaFree(p->d_queue);
+    delete p;
+}
+
+int htc_program_check(htc_program *p, void *stream) {
+    int rc = check_program(p);
+    if (rc) return rc;
+    uint32_t err = 0;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    HTC_CUDA(cudaMemcpyAsync(&err, p->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    HTC_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        HTC_CUDA(cudaMemsetAsync(p->d_err, 0, sizeof(uint32_t), st));
+        HTC_CUDA(cudaStreamSynchronize(st));
+        if (err & ERR_SCENE) return fail(HTC_ERR_SCENE, "scene bytes failed validation (object count or shape index out of range)");
+        return fail(HTC_ERR_SCENE, "device error word set");
+    }
+    return HTC_OK;
+}
+
+int htc_malloc(void **dptr, size_t bytes) {
+    if (!dptr) return fail(HTC_ERR_INVALID, "dptr is NULL");
+    HTC_CUDA(cudaMalloc(dptr, bytes ? bytes : 1));
+    return HTC_OK;
+}
+int htc_free(void *dptr) {
+    HTC_CUDA(cudaFree(dptr));
+    return HTC_OK;
+}
+int htc_memcpy_htod(void *dst, const void *src, size_t bytes, void *stream) {
+    HTC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
+    return HTC_OK;
+}
+int htc_memcpy_dtoh(void *dst, const void *src, size_t bytes, void *stream) {
+    HTC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, reinterpret_cast<cudaStream_t>(stream)));
+    return HTC_OK;
+}
+int htc_memset(void *dst, int value, size_t bytes, void *stream) {
+    HTC_CUDA(cudaMemsetAsync(dst, value, bytes, reinterpret_cast<cudaStream_t>(stream)));
+    return HTC_OK;
+}
+int htc_stream_sync(void *stream) {
+    HTC_CUDA(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+    return HTC_OK;
+}
+
+int htc_render_ex(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                  float *canvas, uint32_t *seeds, uint64_t *stats, void *stream) {
+    uint32_t max_objects = 0;
+    size_t smem = 0;
+    int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
+    if (rc) return rc;
+    dim3 grid((W + 31) / 32, (H + 3) / 4);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint8_t *sc = reinterpret_cast<const uint8_t *>(scene);
+    float4 *cv = reinterpret_cast<float4 *>(canvas);
+    if (p->recipe == HTC_RECIPE_HY)
+        render_plain<RECIPE_HY><<<grid, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+                                                         p->hops, p->flags, cv, seeds, stats, p->d_err);
+    else
+        render_plain<RECIPE_EU><<<grid, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+                                                         p->hops, p->flags, cv, seeds, stats, p->d_err);
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+int htc_render(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size, float *canvas,
+               uint32_t *seeds, void *stream) {
+    return htc_render_ex(p, W, H, scene, scene_size, canvas, seeds, nullptr, stream);
+}
+
+int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                      float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+    uint32_t max_objects = 0;
+    size_t smem = 0;
+    int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
+    if (rc) return rc;
+    if (passes == 0) return HTC_OK;
+    int per_sm = 0;
+    cudaError_t e;
+    if (p->recipe == HTC_RECIPE_HY)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent<RECIPE_HY>, 128, smem);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent<RECIPE_EU>, 128, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)p->num_sms;
+    const uint64_t needed = ((uint64_t)W * H + 127) / 128;
+    if (blocks > needed) blocks = needed;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint8_t *sc = reinterpret_cast<const uint8_t *>(scene);
+    float4 *cv = reinterpret_cast<float4 *>(canvas);
+    if (p->recipe == HTC_RECIPE_HY)
+        render_persistent<RECIPE_HY><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+                                                                          p->hops, passes, p->flags, cv, seeds, stats,
+                                                                          p->d_err, p->d_queue);
+    else
+        render_persistent<RECIPE_EU><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+                                                                          p->hops, passes, p->flags, cv, seeds, stats,
+                                                                          p->d_err, p->d_queue);
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+static unsigned post_blocks(uint32_t n) {
+    uint32_t b = (n + 255) / 256;
+    return b > 148u * 16u ? 148u * 16u : (b ? b : 1u);
+}
+
+int htc_extract(uint32_t W, uint32_t H, uint32_t passes, const float *canvas, float *image, void *stream) {
+    if (!canvas || !image || passes == 0) return fail(HTC_ERR_INVALID, "bad extract arguments");
+    uint32_t n = W * H;
+    k_extract<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        n, (float)passes, reinterpret_cast<const float4 *>(canvas), reinterpret_cast<float4 *>(image));
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+int htc_gamma(uint32_t W, uint32_t H, float gamma, const float *input, float *output, void *stream) {
+    if (!input || !output) return fail(HTC_ERR_INVALID, "bad gamma arguments");
+    uint32_t n = W * H;
+    k_gamma<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        n, gamma, reinterpret_cast<const float4 *>(input), reinterpret_cast<float4 *>(output));
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+int htc_pack(uint32_t W, uint32_t H, const float *image, uint8_t *packed, void *stream) {
+    if (!image || !packed) return fail(HTC_ERR_INVALID, "bad pack arguments");
+    uint32_t n = W * H;
+    k_pack<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        n, reinterpret_cast<const float4 *>(image), reinterpret_cast<uchar4 *>(packed));
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+int htc_extract_gamma_pack(uint32_t W, uint32_t H, uint32_t passes, float gamma, const float *canvas,
+                           uint8_t *packed, void *stream) {
+    if (!canvas || !packed || passes == 0) return fail(HTC_ERR_INVALID, "bad extract_gamma_pack arguments");
+    uint32_t n = W * H;
+    k_extract_gamma_pack<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        n, (float)passes, gamma, reinterpret_cast<const float4 *>(canvas), reinterpret_cast<uchar4 *>(packed));
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+}  // extern "C"

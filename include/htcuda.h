@@ -1,0 +1,125 @@
+/*
+ * htcuda.h -- C ABI of the B200-native hypertrace render path (libhtcuda.so).
+ *
+ * This is the drop-in boundary for the reference's OpenCL dispatch layer: a
+ * `backend_cuda` feature of the `processing` crate binds these symbols where
+ * `backend_ocl` drives the `ocl` crate today (processing/src/context.rs:3-16).
+ * Every entry point returns an int status (HTC_OK = 0, negative on error) and sets a
+ * thread-local message readable with htc_last_error(). No C++ exception crosses the ABI.
+ * Streams are `cudaStream_t` values passed as `void *` (NULL = legacy default stream);
+ * device pointers are plain `cudaMalloc`'d (or torch-owned) addresses.
+ */
+#ifndef HTCUDA_H
+#define HTCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define HTC_OK 0
+#define HTC_ERR_INVALID (-1)      /* bad argument */
+#define HTC_ERR_CUDA (-2)         /* a CUDA runtime call failed */
+#define HTC_ERR_SCENE (-3)        /* scene bytes failed validation (device-side check) */
+#define HTC_ERR_UNSUPPORTED (-4)  /* configuration this build does not serve */
+#define HTC_ERR_BUDGET (-5)       /* admission refused: memory budget exceeded */
+#define HTC_ERR_TIMEOUT (-6)      /* a bounded device wait or work loop gave up */
+
+/* ---------------------------------------------------------------- scene recipes
+ * The scene types the hand-written kernels serve (the Rust types that the reference's
+ * codegen turns into OpenCL C, objects/src/scene.rs:44-67):
+ *   HTC_RECIPE_HY  SceneImpl<Hyperbolic3, Mapped<PointView, Moebius>,
+ *                    Vec<Mapped<Covered<Choice{Plane, Horosphere},
+ *                      Mixture{Colored<Lambertian>, Specular, Emissive<Absorbing>}>, Moebius>>,
+ *                    ConstBg, H>                          (main/examples/hearth.rs:27-41)
+ *   HTC_RECIPE_EU  the same over Euclidean3 with Homogenous3 maps and
+ *                  Choice{Plane, Sphere}                  (main/examples/eu.rs:30-44)
+ */
+#define HTC_RECIPE_HY 1
+#define HTC_RECIPE_EU 2
+
+/* Program flags. */
+#define HTC_FLAG_JITTER_YX 1u  /* first pixel-jitter draw goes to y: the order in which g++
+                                  evaluates random_uniform2's arguments in the reference's
+                                  host build (kernel/ocl/random.cc:15-20); the default is
+                                  the OpenCL order (first draw -> x). */
+
+/* Render statistics written by the *_ex entry points (device buffer of 4 x uint64,
+ * accumulated with atomics; zero it before the launch). */
+#define HTC_STAT_SAMPLES 0       /* completed paths (scene_sample calls) */
+#define HTC_STAT_HOPS 1          /* executed hop iterations (ray bounces) */
+#define HTC_STAT_OBJECT_TESTS 2  /* object detect calls (hops x objects) */
+#define HTC_STAT_HITS 3          /* hops that hit an object */
+
+typedef struct htc_program htc_program;
+
+/* ---------------------------------------------------------------- runtime */
+const char *htc_last_error(void);
+int htc_version(void);
+int htc_device_count(int *count);
+int htc_set_device(int device);
+
+/* Replaces Render::new (processing/src/render.rs:72-100): selects the compiled kernel
+ * family for a scene recipe and light-hop count H (objects/src/scene.rs:21,64).
+ * address_width: 32 or 64 (types/src/config.rs:18-31); double_support must be 0. */
+int htc_program_create(int recipe, uint32_t light_hops, int address_width, int double_support,
+                       uint32_t flags, htc_program **out);
+void htc_program_destroy(htc_program *program);
+/* Reads and clears the device-side error word of the program's last launches
+ * (synchronises `stream`). Returns HTC_OK or HTC_ERR_SCENE / HTC_ERR_TIMEOUT. */
+int htc_program_check(htc_program *program, void *stream);
+
+/* ---------------------------------------------------------------- buffers */
+int htc_malloc(void **dptr, size_t bytes);
+int htc_free(void *dptr);
+int htc_memcpy_htod(void *dst, const void *src, size_t bytes, void *stream);
+int htc_memcpy_dtoh(void *dst, const void *src, size_t bytes, void *stream);
+int htc_memset(void *dst, int value, size_t bytes, void *stream);
+int htc_stream_sync(void *stream);
+
+/* ---------------------------------------------------------------- render
+ * One pass over a width x height canvas: the `render` kernel of
+ * kernel/ocl/render/render.cl:6-27 as enqueued by Render::render
+ * (processing/src/render.rs:102-118): canvas[idx] += (radiance, 1), seeds[idx] advanced.
+ *   scene       device pointer to the serialized scene bytes (EntityBuffer, buffer.rs:14-29)
+ *   scene_size  its size in bytes (bounds every device read of the scene)
+ *   canvas      device float4[width*height];  seeds: device uint32[width*height]
+ * Asynchronous on `stream`; scene validity is reported by htc_program_check. */
+int htc_render(htc_program *program, uint32_t width, uint32_t height, const void *scene,
+               size_t scene_size, float *canvas, uint32_t *seeds, void *stream);
+
+/* `passes` successive passes in one persistent launch. The result is bit-identical to
+ * `passes` htc_render calls: each pixel's samples run in order on one thread, which keeps
+ * its RNG stream, and finished paths are regenerated in place so lanes stay busy.
+ * stats (optional, device uint64[4]) accumulates the HTC_STAT_* counters. */
+int htc_render_passes(htc_program *program, uint32_t width, uint32_t height, const void *scene,
+                      size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
+                      uint64_t *stats, void *stream);
+
+/* htc_render with statistics (the plain one-pass kernel). */
+int htc_render_ex(htc_program *program, uint32_t width, uint32_t height, const void *scene,
+                  size_t scene_size, float *canvas, uint32_t *seeds, uint64_t *stats,
+                  void *stream);
+
+/* ---------------------------------------------------------------- post chain
+ * Extractor (processing/src/canvas.rs:126-135): image = canvas / passes.
+ * GammaFilter (processing/src/filter/gamma.rs:10-19): out = pow(max(in, 0), gamma).
+ * Packer (processing/src/canvas.rs:176-186): u8 = (uchar)(255 * clamp(x, 0, 1)), toward 0. */
+int htc_extract(uint32_t width, uint32_t height, uint32_t passes, const float *canvas,
+                float *image, void *stream);
+int htc_gamma(uint32_t width, uint32_t height, float gamma, const float *input, float *output,
+              void *stream);
+int htc_pack(uint32_t width, uint32_t height, const float *image, uint8_t *packed, void *stream);
+/* The three stages fused in one pass over the canvas (what Pipeline::get_image computes,
+ * processing/src/pipeline.rs:53-62). */
+int htc_extract_gamma_pack(uint32_t width, uint32_t height, uint32_t passes, float gamma,
+                           const float *canvas, uint8_t *packed, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HTCUDA_H */

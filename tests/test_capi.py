@@ -1,0 +1,53 @@
+"""The C ABI library loads without a GPU and exports every symbol include/htcuda.h declares."""
+import os
+import re
+
+import pytest
+
+from hypertrace_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(htc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = _declared("htcuda.h")
+    assert "htc_render" in names and "htc_render_passes" in names and "htc_extract_gamma_pack" in names
+
+
+def test_library_exports_every_declared_symbol(built):
+    lib = _lib.lib()
+    for name in _declared("htcuda.h"):
+        assert hasattr(lib, name), f"libhtcuda.so does not export {name}"
+
+
+def test_binding_covers_header(built):
+    bound = {n for n, _, _ in _lib.SIGNATURES}
+    assert set(_declared("htcuda.h")) <= bound
+
+
+def test_errors_without_device(built):
+    """Argument checks fail loudly with a message (no device needed for these)."""
+    import ctypes
+    h = ctypes.c_void_p()
+    rc = _lib.lib().htc_program_create(99, 4, 32, 0, 0, ctypes.byref(h))
+    assert rc == _lib.HTC_ERR_UNSUPPORTED
+    assert b"recipe" in _lib.lib().htc_last_error()
+    rc = _lib.lib().htc_program_create(1, 0, 32, 0, 0, ctypes.byref(h))
+    assert rc == _lib.HTC_ERR_INVALID
+    rc = _lib.lib().htc_program_create(1, 4, 32, 1, 0, ctypes.byref(h))
+    assert rc == _lib.HTC_ERR_UNSUPPORTED
+    rc = _lib.lib().htc_render(None, 4, 4, None, 0, None, None, None)
+    assert rc == _lib.HTC_ERR_INVALID
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "nope.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _lib.lib()
