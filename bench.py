@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark: Msamples/s and ray-bounces/s of the path-tracing hot path at 1080p hyperbolic.
+
+Workload (one GPU): the 1920x1080 hyperbolic scene of 200 objects (60 % horospheres,
+40 % geodesic planes) placed by random det-1 Moebius maps with translation distance up to 6,
+H = 8 light hops, synthetic and seeded (hypertrace_b200.scene.config2). A step is one
+launch of the persistent kernel rendering `--passes` passes over the whole frame (each pass
+is one sample per pixel); the frame's 256 spp are 256 / passes such steps.
+
+    python bench.py [--gpus N --steps K --warmup W --passes P]
+    python bench.py --impl reference      # the reference's own kernel code on the host CPU
+
+Under torchrun (N > 1) each rank renders its own frame (replicas: the path has no exchange
+step); the reported value is all ranks' samples over the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Msamples/s at 1080p hyperbolic (1920x1080, 200 objects, H=8)"
+UNIT = "Msamples/s"
+
+# Executed FP32 operations per unit of work in the CUDA path (static tally of the source,
+# each add/sub/mul/div/sqrt/log/sin/cos = 1): see DESIGN.md "Roofline".
+FLOPS_PER_OBJECT_TEST = 219     # one inverse ray map (204) + shape distance test lower bound (15)
+FLOPS_PER_HIT_HOP = 936         # winner recompute + map back + interact maps + material
+FLOPS_PER_SAMPLE = 120          # camera ray
+# The reference's own count (two ray maps of 256 ops per candidate: object/mapped.inl:32,34).
+REF_FLOPS_PER_OBJECT_TEST = 527
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--passes", type=int, default=4, help="passes (samples per pixel) per step")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ht_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_baseline(wl, seconds: float, threads: int = 0):
+    """The reference's own kernel code (oracle/_ref, host C++) on this box's cores, on a
+    bounded sample of the workload: chunks of pixels of the frame, one pass each, until
+    `seconds` of wall time are spent. Falls back to the C restatement when _ref is absent."""
+    from oracle import oracle
+    kind = "reference" if oracle.ref_available(32) else "port"
+    cores = threads or os.cpu_count() or 1
+    sc = wl.scene
+    data = sc.to_bytes()
+    W, H = wl.width, wl.height
+    rng = np.random.default_rng(0)
+    chunk = 2048
+    samples = 0
+    from hypertrace_b200.scene import pixel_seeds
+    seeds_all = pixel_seeds(wl.global_seed, W * H)
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        pix = rng.choice(W * H, chunk, replace=False).astype(np.uint32)
+        seeds = seeds_all[pix]
+        flags = oracle.JITTER_YX if kind == "port" else 0
+        r = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds, passes=1, impl=kind, threads=cores,
+                          flags=flags)
+        samples += r.stats["samples"]
+    dt = time.perf_counter() - t0
+    return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{samples} samples (random pixels of the 1920x1080 frame, 1 pass each) in {dt:.1f} s"}
+
+
+def run_reference(args, rank: int):
+    """--impl reference: time the reference's CPU implementation with all host threads."""
+    if rank != 0:
+        return
+    from hypertrace_b200 import scene as S
+    from oracle import oracle
+    wl = S.config2()
+    kind = "reference" if oracle.ref_available(32) else "port"
+    sc = wl.scene
+    data = sc.to_bytes()
+    W, H = wl.width, wl.height
+    cores = os.cpu_count() or 1
+    pix_per_step = 4096
+    rng = np.random.default_rng(1)
+    seeds_all = S.pixel_seeds(wl.global_seed, W * H)
+
+    def step():
+        pix = rng.choice(W * H, pix_per_step, replace=False).astype(np.uint32)
+        r = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds_all[pix], passes=1, impl=kind,
+                          threads=cores, flags=0 if kind == "reference" else oracle.JITTER_YX)
+        return r.stats
+
+    for _ in range(args.warmup):
+        step()
+    samples = hops = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = step()
+        samples += st["samples"]
+        hops += st["hops"]
+    dt = time.perf_counter() - t0
+    value = samples / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "width": W, "height": H, "objects": sc.n_objects, "hops": sc.hops,
+                   "pixels_per_step": pix_per_step, "passes_per_step": 1},
+        "ray_bounces_per_s": hops / dt,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{args.steps} steps x {pix_per_step} random pixels x 1 pass of the 1080p frame"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU side
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import ctypes
+    from hypertrace_b200 import scene as S
+    from hypertrace_b200 import processing as P
+    from hypertrace_b200 import _lib
+    from hypertrace_b200 import build as hb
+
+    hb.build()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    wl = S.config2()
+    sc = wl.scene
+    W, H = wl.width, wl.height
+    ctx = P.Context(local_rank)
+    dev = ctx.device
+    stream = torch.cuda.current_stream(dev)
+    buf = P.EntityBuffer(ctx, sc)
+    canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed + 7919 * rank)
+    render = P.Render(ctx, sc.recipe, sc.hops)
+    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    # FP32 peak of this GPU (roofline denominator): FMA probe, best of several launches.
+    probe_blocks = 148 * 8
+    scratch = torch.empty(probe_blocks * 256, dtype=torch.float32, device=dev)
+    flops = ctypes.c_double()
+    best = 0.0
+    for i in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.call("htc_fp32_probe", scratch.data_ptr(), probe_blocks, 4096, ctypes.byref(flops), stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))
+    fp32_peak_tflops = best / 1e12
+
+    def step(with_stats):
+        render.render_passes(buf, canvas, args.passes, stats=stats if with_stats else None, sync=False)
+
+    for _ in range(args.warmup):
+        step(False)
+    _lib.call("htc_program_check", render.handle, stream.cuda_stream)
+
+    # ---------------- timed region: K steps, device time per launch, L2 flushed in between
+    stats.zero_()
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    times = []
+    for _ in range(args.steps):
+        l2_flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(True)
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    _lib.call("htc_program_check", render.handle, stream.cuda_stream)
+    launch_ms = [a.elapsed_time(b) for a, b in times]
+    dev_s = sum(launch_ms) * 1e-3
+    st = stats.cpu().numpy().astype(np.float64)
+    samples, hops, tests, hits = st
+    t = torch.tensor([dev_s], dtype=torch.float64, device=dev)
+    tot = torch.tensor([samples, hops], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    max_s = float(t.item())
+    all_samples, all_hops = [float(x) for x in tot.cpu()]
+    value = all_samples / max_s / 1e6
+
+    # roofline of the persistent kernel (one launch per step)
+    exec_flops = tests * FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
+    ref_flops = tests * REF_FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
+    per_launch_s = dev_s / args.steps
+    achieved = exec_flops / args.steps / per_launch_s / 1e12
+
+    # ---------------- plain kernel (one pass per launch) on the same frame, for comparison
+    plain = None
+    if rank == 0:
+        stats.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.passes):
+            render.render(buf, canvas, stats=stats, sync=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ps = stats.cpu().numpy()
+        plain = {"value": float(ps[0]) / ms / 1e3, "unit": UNIT, "ms_per_pass": ms / args.passes,
+                 "ray_bounces_per_s": float(ps[1]) / ms * 1e3}
+
+    # ---------------- e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pipe = P.Pipeline(ctx, (W, H), sc, global_seed=wl.global_seed + 7919 * rank)
+        host_scene = torch.frombuffer(bytearray(sc.to_bytes()), dtype=torch.uint8).pin_memory()
+        host_image = torch.empty(W * H * 4, dtype=torch.uint8).pin_memory()
+        for _ in range(2):
+            pipe.render(args.passes)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            pipe.scene_buffer.tensor.copy_(host_scene, non_blocking=True)      # set_scene upload
+            pipe.render_.render_passes(pipe.scene_buffer, pipe.canvas, args.passes, sync=False)
+            _lib.call("htc_extract_gamma_pack", W, H, max(pipe.canvas.passes, 1), ctypes.c_float(1 / 2.2),
+                      pipe.canvas.image.data_ptr(), pipe.packed.data_ptr(), stream.cuda_stream)
+            host_image.copy_(pipe.packed, non_blocking=True)                  # get_image read-back
+            stream.synchronize()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        e2e_s = ev0.elapsed_time(ev1) * 1e-3
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_samples = float(W * H * args.passes * args.steps * world)
+        e2e = {"value": e2e_samples / float(tt.item()) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(host_scene.numel()), "d2h_bytes_per_step": int(host_image.numel()),
+               "wall_s": time.perf_counter() - t0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_s / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl.name, "width": W, "height": H, "objects": sc.n_objects, "hops": sc.hops,
+                       "passes_per_step": args.passes, "kernel": "render_persistent",
+                       "parallelism": f"replicas{world}",
+                       "l2": "flushed between steps (256 MB device write outside the timed events)"},
+            "ray_bounces_per_s": all_hops / max_s,
+            "hops_per_sample": hops / max(samples, 1),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak_tflops if fp32_peak_tflops else None, "traffic": None,
+                         "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",
+                         "flops_per_launch": exec_flops / args.steps,
+                         "reference_count_tflops": ref_flops / args.steps / per_launch_s / 1e12},
+            "plain": plain,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": args.steps,
+            "wall_s_timed": t_wall,
+            "launch_ms": [round(x, 3) for x in launch_ms],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

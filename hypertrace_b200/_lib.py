@@ -53,6 +53,7 @@ SIGNATURES = [
     ("htc_gamma", _i, [_u32, _u32, _f, _vp, _vp, _vp]),
     ("htc_pack", _i, [_u32, _u32, _vp, _vp, _vp]),
     ("htc_extract_gamma_pack", _i, [_u32, _u32, _u32, _f, _vp, _vp, _vp]),
+    ("htc_fp32_probe", _i, [_vp, _u32, _i, ctypes.POINTER(ctypes.c_double), _vp]),
 ]
 
 

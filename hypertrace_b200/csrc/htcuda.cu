@@ -345,6 +345,23 @@ __global__ void k_extract_gamma_pack(uint32_t n, float passes, float g, const fl
     }
 }
 
+// ============================================================================ calibration
+// FP32 FMA throughput probe: independent FMA chains per thread, enough warps to fill every
+// scheduler. 2 flops per FMA; the result is written so nothing is dead code.
+__global__ void __launch_bounds__(256) k_fma_probe(float *out, int iters) {
+    float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+    float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+
 // ============================================================================ C ABI
 static int check_program(const htc_program *p) {
     if (!p) return fail(HTC_ERR_INVALID, "program is NULL");
@@ -583,6 +600,14 @@ int htc_extract_gamma_pack(uint32_t W, uint32_t H, uint32_t passes, float gamma,
     k_extract_gamma_pack<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         n, (float)passes, gamma, reinterpret_cast<const float4 *>(canvas), reinterpret_cast<uchar4 *>(packed));
     HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+int htc_fp32_probe(float *scratch, uint32_t blocks, int iters, double *flops, void *stream) {
+    if (!scratch || !flops || blocks == 0 || iters <= 0) return fail(HTC_ERR_INVALID, "bad probe arguments");
+    k_fma_probe<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(scratch, iters);
+    HTC_CUDA(cudaGetLastError());
+    *flops = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)blocks;
     return HTC_OK;
 }
 

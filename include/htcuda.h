@@ -118,6 +118,13 @@ int htc_pack(uint32_t width, uint32_t height, const float *image, uint8_t *packe
 int htc_extract_gamma_pack(uint32_t width, uint32_t height, uint32_t passes, float gamma,
                            const float *canvas, uint8_t *packed, void *stream);
 
+/* ---------------------------------------------------------------- calibration
+ * FP32 FMA throughput probe used as the roofline denominator of the render kernels
+ * (they are FP32-issue bound). Launches `blocks` x 256 threads of independent FMA chains;
+ * `scratch` is a device float[blocks*256]; *flops receives the flop count of the launch
+ * (2 per FMA). Time it with events on `stream`. No counterpart in the reference. */
+int htc_fp32_probe(float *scratch, uint32_t blocks, int iters, double *flops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
