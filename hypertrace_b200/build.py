@@ -58,5 +58,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
+SELFTEST_SRC = os.path.join(ROOT, "tests", "cuda", "ht_selftest.cu")
+SELFTEST_OUT = os.path.join(ROOT, "tests", "cuda", "libht_selftest.so")
+
+
+def build_selftest(force: bool = False) -> str:
+    """Test-only device unit tests (tests/cuda/ht_selftest.cu), same flags as the library."""
+    if not os.path.exists(SELFTEST_SRC):
+        return ""
+    srcs = sources() + [SELFTEST_SRC]
+    if not force and os.path.exists(SELFTEST_OUT) and all(os.path.getmtime(s) <= os.path.getmtime(SELFTEST_OUT) for s in srcs):
+        return SELFTEST_OUT
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", SELFTEST_OUT, SELFTEST_SRC]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+    return SELFTEST_OUT
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -60,12 +60,51 @@ HT_D Q4 q_add(Q4 a, Q4 b) { return q4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w
 HT_D Q4 q_sub(Q4 a, Q4 b) { return q4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
 HT_D Q4 q_addc(Q4 a, C2 b) { return q4(a.x + b.x, a.y + b.y, a.z + 0.0f, a.w + 0.0f); }  // + q_new(c, C0)
 
+// ------------------------------------------------------------------- division
+// Correctly rounded quotients that share one reciprocal (Markstein's correction step):
+//   y = RN(1/b),  q0 = RN(a*y),  r = a - b*q0 (exact with an FMA),  q = RN(q0 + r*y) = RN(a/b)
+// (P. Markstein, "IA-64 and Elementary Functions", 2000; Muller et al., "Handbook of
+// Floating-Point Arithmetic", 2nd ed., section 4.7, Markstein's theorem). The identity
+// needs every intermediate to be a normal number, so each quotient checks that |q0| lies in
+// [2^-60, 2^60] (or a == 0, where q0 already carries the IEEE sign of zero) and each divisor
+// that |b| does; a group with any value outside redoes its divisions with IEEE division.
+// tests/test_gpu_math.py compares qdiv with IEEE division on billions of inputs.
+struct Rcp { float b, y; };
+HT_D bool in_safe_range(float x) {
+    const float ax = fabsf(x);
+    return ax >= 0x1p-60f && ax <= 0x1p60f;
+}
+HT_D Rcp rcp_of(float b, bool &bad) {
+    bad |= !in_safe_range(b);
+    Rcp r;
+    r.b = b;
+    r.y = __frcp_rn(b);
+    return r;
+}
+HT_D float qdiv(float a, const Rcp &r, bool &bad) {
+    const float q0 = a * r.y;
+    const float e = fmaf(-r.b, q0, a);
+    const float q = fmaf(e, r.y, q0);
+    bad |= (a != 0.0f) & !in_safe_range(q0);
+    return q0 == 0.0f ? q0 : q;
+}
+HT_D Q4 qdiv4(Q4 a, const Rcp &r, bool &bad) {
+    return q4(qdiv(a.x, r, bad), qdiv(a.y, r, bad), qdiv(a.z, r, bad), qdiv(a.w, r, bad));
+}
+// normalize4 through one correctly rounded reciprocal of the length.
+HT_D Q4 normalize4_fast(Q4 a, bool &bad) {
+    float l = sqrtf(dot4(a, a));
+    Rcp r = rcp_of(l, bad);
+    return qdiv4(a, r, bad);
+}
+
 // ------------------------------------------------------------------- Moebius
 // mo_apply_q and mo_deriv_q (kernel/ocl/transform/moebius.cc:20-42) share the numerator u,
 // the denominator d, |d|^2 and q_inverse(d) = conj(d) / |d|^2.
 struct HyRay { Q4 p, v; };
 
-HT_D HyRay ray_hy_map(const Mo &m, Q4 p, Q4 v) {
+// Reference evaluation with IEEE division everywhere (the fallback of ray_hy_map).
+__device__ __noinline__ HyRay ray_hy_map_ieee(const Mo m, const Q4 p, const Q4 v) {
     Q4 u = q_addc(cq_mul(m.a, p), m.b);
     Q4 d = q_addc(cq_mul(m.c, p), m.d);
     float d2 = dot4(d, d);
@@ -84,7 +123,32 @@ HT_D HyRay ray_hy_map(const Mo &m, Q4 p, Q4 v) {
     o.v = normalize4(normalize4(deriv));   // mo_apply_dir normalizes, ray_map.inl:19 again
     return o;
 }
+
+// ray_<hy>_map (geometry/ray_map.inl:15-21): the nine divisions by |d|^2 share one
+// reciprocal, each normalize shares one; results are bit-identical to ray_hy_map_ieee.
+HT_D HyRay ray_hy_map(const Mo &m, Q4 p, Q4 v) {
+    bool bad = false;
+    Q4 u = q_addc(cq_mul(m.a, p), m.b);
+    Q4 d = q_addc(cq_mul(m.c, p), m.d);
+    float d2 = dot4(d, d);
+    Rcp rd = rcp_of(d2, bad);
+    Q4 di = qdiv4(q4(d.x, -d.y, -d.z, -d.w), rd, bad);
+    HyRay o;
+    o.p = q_mul(u, di);
+    Q4 g1 = q_mul(cq_mul(m.a, v), di);
+    Q4 cv = cq_mul(m.c, v);
+    Q4 g21 = q_conj(cv);
+    float k = qdiv(2.0f * dot4(d, cv), rd, bad);
+    Q4 dc = q_conj(d);
+    Q4 g22 = q4(k * dc.x, k * dc.y, k * dc.z, k * dc.w);
+    Q4 g2 = q_mul(u, qdiv4(q_sub(g21, g22), rd, bad));
+    Q4 deriv = q_add(g1, g2);
+    o.v = normalize4_fast(normalize4_fast(deriv, bad), bad);
+    if (bad) return ray_hy_map_ieee(m, p, v);
+    return o;
+}
 // Camera map (view/mapped.inl:20-26): direction = mo_apply_dir (one normalize), then start.
+// Once per sample, so plain IEEE division.
 HT_D HyRay view_hy_map(const Mo &m, Q4 p, Q4 v) {
     Q4 u = q_addc(cq_mul(m.a, p), m.b);
     Q4 d = q_addc(cq_mul(m.c, p), m.d);
@@ -139,12 +203,19 @@ HT_D Hom hom3_inverse(const Hom &m) {
 }
 
 // ------------------------------------------------------------------- hyperbolic geometry
-// kernel/ocl/geometry/hyperbolic.cc:20-33
-HT_D float hy_distance(Q4 a, Q4 b) {
+// kernel/ocl/geometry/hyperbolic.cc:20-33, split in two: hy_distance(a, b) =
+// hy_dist_from_x(hy_x(a, b)). The object scan compares x and evaluates the logarithm only
+// for a candidate that can be nearer than the current one; that equals comparing the
+// distances because hy_dist_from_x, as compiled here, is non-decreasing on [1, inf]
+// (checked exhaustively over every float in tests/test_gpu_math.py).
+HT_D float hy_x(Q4 a, Q4 b) {
     Q4 d = q_sub(a, b);
-    float x = 1.0f + dot4(d, d) / (2.0f * a.z * b.z);
+    return 1.0f + dot4(d, d) / (2.0f * a.z * b.z);
+}
+HT_D float hy_dist_from_x(float x) {
     return logf(x + sqrtf(x * x - 1.0f));
 }
+HT_D float hy_distance(Q4 a, Q4 b) { return hy_dist_from_x(hy_x(a, b)); }
 HT_D Q4 hy_dir_at(Q4 p, Q4 d, Q4 h) {
     float lpxy = sqrtf(dot2(p.x - h.x, p.y - h.y, p.x - h.x, p.y - h.y));
     float ldxy = sqrtf(dot2(d.x, d.y, d.x, d.y));

@@ -133,8 +133,9 @@ struct StagedScene {
 // -------------------------------------------------------------------------- hyperbolic
 struct HyPath { Q4 p, v; };
 
-// Distance-only plane test (shape/hy/plane.cc:4-37 without the direction update).
-HT_D float plane_hy_dist(Q4 p, Q4 d) {
+// Plane test up to the hit point (shape/hy/plane.cc:4-37 without the direction update);
+// returns x of the hit distance (see hy_x), or -1 on a miss.
+HT_D float plane_hy_x(Q4 p, Q4 d) {
     float pd = dot4(p, d);
     if (fabsf(pd) < EPSF) return -1.0f;
     float s = 1.0f - dot4(p, p);
@@ -144,10 +145,10 @@ HT_D float plane_hy_dist(Q4 p, Q4 d) {
     float pxy2 = dot2(hx, hy, hx, hy);
     if (pxy2 > 1.0f) return -1.0f;
     Q4 h = q4(hx, hy, sqrtf(1.0f - pxy2), 0.0f);
-    return hy_distance(p, h);
+    return hy_x(p, h);
 }
-// Distance-only horosphere test (shape/hy/horosphere.cc:4-34).
-HT_D float horosphere_dist(Q4 p, Q4 d, bool repeat) {
+// Horosphere test up to the hit point (shape/hy/horosphere.cc:4-34); x or -1.
+HT_D float horosphere_x(Q4 p, Q4 d, bool repeat) {
     float dxy = sqrtf(dot2(d.x, d.y, d.x, d.y));
     if (p.z < dxy) return -1.0f;
     float dt = sqrtf(p.z * p.z - dxy * dxy);
@@ -159,7 +160,7 @@ HT_D float horosphere_dist(Q4 p, Q4 d, bool repeat) {
     }
     t /= dxy * dxy;
     Q4 h = q4(p.x + d.x * t, p.y + d.y * t, 1.0f, 0.0f);
-    return hy_distance(p, h);
+    return hy_x(p, h);
 }
 // Full tests for the winning object: hit point, transported direction, local normal.
 HT_D void plane_hy_hit(Q4 p, Q4 d, HyPath &hit, Q4 &normal) {
@@ -205,25 +206,32 @@ HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint
 // `hit` reports whether the scan found an object (for the hop statistics).
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
                  Col &intensity, Col &emission, bool &hit) {
+    // Nearest hit with ties to the lowest index (object/vector.inl:37-50), comparing
+    // x = cosh(distance) and taking the logarithm only when x can win.
     float min_dist = -1.0f;
+    float min_x = __int_as_float(0x7f800000);   // +inf
     uint32_t kmin = 0;
     const Q4 p = ray.p, v = ray.v;
     for (uint32_t k = 0; k < s.n; ++k) {
         const uint32_t shape = s.shape[k];
         const bool repeat = (k == prev_hash);
-        float dist = -1.0f;
+        float x = -1.0f;
         if (shape == 0) {
             if (!repeat) {  // a geodesic plane is never hit twice in a row (plane.cc:6-9)
                 HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
-                dist = plane_hy_dist(l.p, l.v);
+                x = plane_hy_x(l.p, l.v);
             }
         } else {
             HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
-            dist = horosphere_dist(l.p, l.v, repeat);
+            x = horosphere_x(l.p, l.v, repeat);
         }
-        if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
-            min_dist = dist;
-            kmin = k;
+        if (x >= 1.0f && x <= min_x) {
+            const float dist = hy_dist_from_x(x);
+            if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+                min_dist = dist;
+                min_x = x;
+                kmin = k;
+            }
         }
     }
     if (!(min_dist > -EPSF)) {

@@ -40,6 +40,17 @@ static int cuda_fail(cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+// Minimum resident blocks per SM requested from ptxas for the render kernels (register cap).
+// Six 128-thread blocks per SM (80 registers) measured fastest for both kernels: the scan
+// is latency-bound on dependent FP32 chains, so resident warps matter more than the few
+// spilled values of the cold per-path state.
+#ifndef HT_PERSIST_MINB
+#define HT_PERSIST_MINB 6
+#endif
+#ifndef HT_PLAIN_MINB
+#define HT_PLAIN_MINB 6
+#endif
+
 // Device error word bits.
 constexpr uint32_t ERR_SCENE = 1u;
 constexpr uint32_t ERR_SMEM = 2u;
@@ -145,9 +156,10 @@ __device__ __forceinline__ void pixel_pos(uint32_t x, uint32_t y, uint32_t W, ui
     size = 2.0f / __uint2float_rn(H);
 }
 
-__device__ __forceinline__ void flush_stats(uint64_t *stats, uint64_t samples, uint64_t hops,
-                                            uint64_t hits, uint32_t n_objects) {
+__device__ __forceinline__ void flush_stats(uint64_t *stats, uint32_t samples32, uint32_t hops32,
+                                            uint32_t hits32, uint32_t n_objects) {
     if (!stats) return;
+    uint64_t samples = samples32, hops = hops32, hits = hits32;
     for (int off = 16; off > 0; off >>= 1) {
         samples += __shfl_down_sync(0xffffffffu, samples, off);
         hops += __shfl_down_sync(0xffffffffu, hops, off);
@@ -163,7 +175,7 @@ __device__ __forceinline__ void flush_stats(uint64_t *stats, uint64_t samples, u
 
 // ============================================================================ plain
 template <int R>
-__global__ void __launch_bounds__(128) render_plain(
+__global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
     uint32_t W, uint32_t H, uint32_t hops, uint32_t flags, float4 *__restrict__ canvas,
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err) {
@@ -178,7 +190,7 @@ __global__ void __launch_bounds__(128) render_plain(
     const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
     const uint32_t y = blockIdx.y * 4 + (threadIdx.x >> 5);
     const bool inside = x < W && y < H;
-    uint64_t n_samples = 0, n_hops = 0, n_hits = 0;
+    uint32_t n_samples = 0, n_hops = 0, n_hits = 0;
     if (inside) {
         const uint32_t idx = x + W * y;
         float px, py, size;
@@ -208,7 +220,7 @@ __global__ void __launch_bounds__(128) render_plain(
 constexpr uint32_t NO_PIXEL = 0xFFFFFFFFu;
 
 template <int R>
-__global__ void __launch_bounds__(128) render_persistent(
+__global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
     uint32_t W, uint32_t H, uint32_t hops, uint32_t passes, uint32_t flags,
     float4 *__restrict__ canvas, uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err,
@@ -222,7 +234,7 @@ __global__ void __launch_bounds__(128) render_persistent(
 
     const uint32_t total = W * H;
     const uint32_t lane = threadIdx.x & 31;
-    uint64_t n_samples = 0, n_hops = 0, n_hits = 0;
+    uint32_t n_samples = 0, n_hops = 0, n_hits = 0;
 
     if (staged) {
         uint32_t pixel = NO_PIXEL;
