@@ -32,7 +32,8 @@ UNIT = "Msamples/s"
 
 # Executed FP32 operations per unit of work in the CUDA path (static tally of the source,
 # each add/sub/mul/div/sqrt/log/sin/cos = 1): see DESIGN.md "Roofline".
-FLOPS_PER_OBJECT_TEST = 219     # one inverse ray map (204) + shape distance test lower bound (15)
+FLOPS_PER_EXACT_TEST = 219      # one inverse ray map (204) + shape distance test lower bound (15)
+FLOPS_PER_BOUND_TEST = 18       # world-space distance bound of one object (hops x objects of them)
 FLOPS_PER_HIT_HOP = 936         # winner recompute + map back + interact maps + material
 FLOPS_PER_SAMPLE = 120          # camera ray
 # The reference's own count (two ray maps of 256 ops per candidate: object/mapped.inl:32,34).
@@ -210,7 +211,7 @@ def main():
     buf = P.EntityBuffer(ctx, sc)
     canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed + 7919 * rank)
     render = P.Render(ctx, sc.recipe, sc.hops)
-    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    stats = torch.zeros(8, dtype=torch.int64, device=dev)
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     # FP32 peak of this GPU (roofline denominator): FMA probe, best of several launches.
@@ -260,7 +261,7 @@ def main():
     launch_ms = [a.elapsed_time(b) for a, b in times]
     dev_s = sum(launch_ms) * 1e-3
     st = stats.cpu().numpy().astype(np.float64)
-    samples, hops, tests, hits = st
+    samples, hops, tests, hits, exact = st[:5]
     t = torch.tensor([dev_s], dtype=torch.float64, device=dev)
     tot = torch.tensor([samples, hops], dtype=torch.float64, device=dev)
     if world > 1:
@@ -271,7 +272,8 @@ def main():
     value = all_samples / max_s / 1e6
 
     # roofline of the persistent kernel (one launch per step)
-    exec_flops = tests * FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
+    exec_flops = (exact * FLOPS_PER_EXACT_TEST + tests * FLOPS_PER_BOUND_TEST + hits * FLOPS_PER_HIT_HOP
+                  + samples * FLOPS_PER_SAMPLE)
     ref_flops = tests * REF_FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
     per_launch_s = dev_s / args.steps
     achieved = exec_flops / args.steps / per_launch_s / 1e12
@@ -340,6 +342,7 @@ def main():
                        "l2": "flushed between steps (256 MB device write outside the timed events)"},
             "ray_bounces_per_s": all_hops / max_s,
             "hops_per_sample": hops / max(samples, 1),
+            "exact_tests_per_hop": exact / max(hops, 1),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak_tflops if fp32_peak_tflops else None, "traffic": None,
                          "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",

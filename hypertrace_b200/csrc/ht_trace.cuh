@@ -123,6 +123,7 @@ HT_D bool mixture_interact(const Material &m, uint32_t &rng, V3 normal, V3 &dir,
 struct StagedScene {
     const float4 *inv;       // shared, 2 per object
     const uint32_t *shape;   // shared
+    const float4 *bound;     // shared, 1 per object: world-space form for distance bounds
     const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials)
     uint32_t n;
     float fov;
@@ -204,33 +205,116 @@ HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint
 
 // One hop (one iteration of render/scene.inl:25-41). Returns true while the path goes on.
 // `hit` reports whether the scan found an object (for the hop statistics).
+// ---------------------------------------------------------------- distance bounds
+// Any hit on object k lies on the object, so its distance is at least the distance from
+// the ray start to the object. With the world-space form of each object (staged once per
+// launch, stage_bound below) that bound costs a few FMAs, and objects whose bound exceeds
+// the best distance found so far -- widened by CULL_REL and CULL_ABS, far above the float
+// error of either side -- cannot become the nearest hit and are not tested. This changes
+// which objects are evaluated, never the result.
+//   geodesic plane:  normalised Hermitian form (A, B, C), |B|^2 - A C = 1, of the world
+//                    plane; Q(p) = A(|z|^2 + t^2) + 2 Re(B conj z) + C,
+//                    sinh(dist(p, plane)) = |Q| / (2 t)
+//   horosphere:      local height t' = t / (|n21 z + n22|^2 + |n21|^2 t^2) with N = M^-1
+//                    normalised to det 1; dist(p, horosphere) = |ln t'|
+// z = p.x + i p.y, t = p.z. Culling is off for objects with large map entries (NaN
+// records never cull) and for ray starts outside a well-conditioned box.
+constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
+
+struct Cull { float S, E; };   // sinh(threshold), exp(threshold); +inf = no culling
+
+// World-space bound record of one object from its f32 map M, in FP64 (once per launch).
+// N = adj(M) maps world to local (c22_inverse_n, matrix_complex.cc:60-65).
+HT_D float4 stage_bound(const Mo &m, uint32_t shape) {
+    const double ar = m.a.x, ai = m.a.y, br = m.b.x, bi = m.b.y;
+    const double cr = m.c.x, ci = m.c.y, dr = m.d.x, di = m.d.y;
+    const double det_r = (ar * dr - ai * di) - (br * cr - bi * ci);
+    const double det_i = (ar * di + ai * dr) - (br * ci + bi * cr);
+    const double adet = sqrt(det_r * det_r + det_i * det_i);
+    const double maxe = fmax(fmax(fabs(ar) + fabs(ai), fabs(br) + fabs(bi)), fmax(fabs(cr) + fabs(ci), fabs(dr) + fabs(di)));
+    const float nan = __int_as_float(0x7fc00000);
+    if (!(maxe <= 32.0 && adet >= 0.5 && adet <= 2.0)) return make_float4(nan, nan, nan, nan);
+    // N = [[n11, n12], [n21, n22]] = [[d, -b], [-c, a]]
+    const double n11r = dr, n11i = di, n12r = -br, n12i = -bi, n21r = -cr, n21i = -ci, n22r = ar, n22i = ai;
+    if (shape == 0) {
+        const double A = (n11r * n11r + n11i * n11i) - (n21r * n21r + n21i * n21i);
+        // B = conj(n11) n12 - conj(n21) n22
+        const double Br = (n11r * n12r + n11i * n12i) - (n21r * n22r + n21i * n22i);
+        const double Bi = (n11r * n12i - n11i * n12r) - (n21r * n22i - n21i * n22r);
+        const double C = (n12r * n12r + n12i * n12i) - (n22r * n22r + n22i * n22i);
+        return make_float4((float)(A / adet), (float)(Br / adet), (float)(Bi / adet), (float)(C / adet));
+    }
+    const double k = 1.0 / sqrt(adet);
+    return make_float4((float)(n21r * k), (float)(n21i * k), (float)(n22r * k), (float)(n22i * k));
+}
+
+HT_D bool cull_point_ok(Q4 p) {
+    return p.z >= 0x1p-20f && p.z <= 0x1p20f && fabsf(p.x) + fabsf(p.y) <= 0x1p10f * p.z &&
+           fabsf(p.w) <= 1e-3f * p.z;
+}
+HT_D Cull cull_from_dist(float d) {
+    const float thr = fmaf(d, 1.0f + CULL_REL, CULL_ABS);
+    Cull c;
+    c.S = sinhf(thr);
+    c.E = expf(thr);
+    return c;
+}
+// true when object k provably cannot be hit nearer than the current threshold
+HT_D bool culled(float4 b, uint32_t shape, Q4 p, const Cull &c) {
+    const float x = p.x, y = p.y, t = p.z;
+    if (shape == 0) {
+        const float r2 = fmaf(x, x, fmaf(y, y, t * t));
+        const float q = fmaf(b.x, r2, fmaf(2.0f * b.y, x, fmaf(2.0f * b.z, y, b.w)));
+        const float err = 1e-5f * fmaf(fabsf(b.x), r2, fmaf(2.0f, fabsf(b.y * x) + fabsf(b.z * y), fabsf(b.w)));
+        return fabsf(q) - err > 2.0f * t * c.S;
+    } else {
+        const float re = fmaf(b.x, x, fmaf(-b.y, y, b.z));
+        const float im = fmaf(b.x, y, fmaf(b.y, x, b.w));
+        const float cc = fmaf(b.x, b.x, b.y * b.y);
+        const float den = fmaf(re, re, fmaf(im, im, cc * t * t));
+        const float sz = (fabsf(b.x) + fabsf(b.y)) * (fabsf(x) + fabsf(y)) + fabsf(b.z) + fabsf(b.w);
+        const float err = 1e-5f * fmaf(sz, sz, cc * t * t);
+        return t > c.E * (den + err) || t * c.E < den - err;
+    }
+}
+
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
-                 Col &intensity, Col &emission, bool &hit) {
+                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact) {
     // Nearest hit with ties to the lowest index (object/vector.inl:37-50), comparing
-    // x = cosh(distance) and taking the logarithm only when x can win.
+    // x = cosh(distance) and taking the logarithm only when x can win, and skipping
+    // objects whose distance bound rules them out.
     float min_dist = -1.0f;
     float min_x = __int_as_float(0x7f800000);   // +inf
     uint32_t kmin = 0;
     const Q4 p = ray.p, v = ray.v;
-    for (uint32_t k = 0; k < s.n; ++k) {
-        const uint32_t shape = s.shape[k];
-        const bool repeat = (k == prev_hash);
-        float x = -1.0f;
-        if (shape == 0) {
-            if (!repeat) {  // a geodesic plane is never hit twice in a row (plane.cc:6-9)
-                HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
-                x = plane_hy_x(l.p, l.v);
-            }
-        } else {
-            HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
-            x = horosphere_x(l.p, l.v, repeat);
+    const bool can_cull = cull_point_ok(p);
+    Cull cull;
+    cull.S = cull.E = __int_as_float(0x7f800000);
+    for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
+        const uint32_t cn = min(32u, s.n - c0);
+        uint32_t mask = 0;
+        for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads
+            const uint32_t k = c0 + j;
+            if (!can_cull || !culled(s.bound[k], s.shape[k], p, cull)) mask |= 1u << j;
         }
-        if (x >= 1.0f && x <= min_x) {
-            const float dist = hy_dist_from_x(x);
-            if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
-                min_dist = dist;
-                min_x = x;
-                kmin = k;
+        while (mask) {   // this lane's candidates, in index order
+            const uint32_t k = c0 + (__ffs(mask) - 1);
+            mask &= mask - 1;
+            const uint32_t shape = s.shape[k];
+            if (can_cull && culled(s.bound[k], shape, p, cull)) continue;
+            const bool repeat = (k == prev_hash);
+            if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
+            ++n_exact;
+            HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+            const float x = shape == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, repeat);
+            if (x >= 1.0f && x <= min_x) {
+                const float dist = hy_dist_from_x(x);
+                if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+                    min_dist = dist;
+                    min_x = x;
+                    kmin = k;
+                    cull = cull_from_dist(dist);
+                }
             }
         }
     }
@@ -302,7 +386,8 @@ HT_D EuPath camera_eu(const StagedScene &s, float px, float py, float size, uint
 }
 
 HT_D bool hop_eu(const StagedScene &s, EuPath &ray, uint32_t &rng, uint32_t &prev_hash,
-                 Col &intensity, Col &emission, bool &hit) {
+                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact) {
+    n_exact += s.n;
     float min_dist = -1.0f;
     uint32_t kmin = 0;
     const V3 p = ray.p, v = ray.v;

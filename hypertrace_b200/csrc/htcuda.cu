@@ -72,7 +72,7 @@ struct htc_program {
 template <int R>
 __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t max_objects,
                             int address_width, uint32_t *err, StagedScene &s, float4 *s_inv,
-                            uint32_t *s_shape, uint32_t *s_hdr) {
+                            float4 *s_bound, uint32_t *s_shape, uint32_t *s_hdr) {
     using L = Layout<R>;
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         uint32_t ok = 1;
@@ -105,9 +105,11 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
         if (shape > 1) bad = true;
         s_shape[k] = shape;
         if (R == RECIPE_HY) {
-            Mo inv = mo_inverse(load_mo(obj));
+            const Mo fwd = load_mo(obj);
+            Mo inv = mo_inverse(fwd);
             s_inv[2 * k] = make_float4(inv.a.x, inv.a.y, inv.b.x, inv.b.y);
             s_inv[2 * k + 1] = make_float4(inv.c.x, inv.c.y, inv.d.x, inv.d.y);
+            s_bound[k] = stage_bound(fwd, shape);
         } else {
             Hom inv = hom3_inverse(load_hom(obj));
             s_inv[2 * k] = make_float4(inv.shift.x, inv.shift.y, inv.shift.z, 0.0f);
@@ -120,6 +122,7 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
         return false;
     }
     s.inv = s_inv;
+    s.bound = s_bound;
     s.shape = s_shape;
     s.objects = scene + L::OBJECTS;
     s.n = n;
@@ -143,9 +146,10 @@ __device__ __forceinline__ typename PathOf<R>::T camera(const StagedScene &s, fl
 }
 template <int R>
 __device__ __forceinline__ bool hop(const StagedScene &s, typename PathOf<R>::T &ray, uint32_t &rng,
-                                    uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit) {
-    if constexpr (R == RECIPE_HY) return hop_hy(s, ray, rng, prev_hash, intensity, emission, hit);
-    else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit);
+                                    uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit,
+                                    uint32_t &n_exact) {
+    if constexpr (R == RECIPE_HY) return hop_hy(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
+    else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
 }
 
 // Pixel centre and size (render.cl:12-18).
@@ -157,19 +161,21 @@ __device__ __forceinline__ void pixel_pos(uint32_t x, uint32_t y, uint32_t W, ui
 }
 
 __device__ __forceinline__ void flush_stats(uint64_t *stats, uint32_t samples32, uint32_t hops32,
-                                            uint32_t hits32, uint32_t n_objects) {
+                                            uint32_t hits32, uint32_t exact32, uint32_t n_objects) {
     if (!stats) return;
-    uint64_t samples = samples32, hops = hops32, hits = hits32;
+    uint64_t samples = samples32, hops = hops32, hits = hits32, exact = exact32;
     for (int off = 16; off > 0; off >>= 1) {
         samples += __shfl_down_sync(0xffffffffu, samples, off);
         hops += __shfl_down_sync(0xffffffffu, hops, off);
         hits += __shfl_down_sync(0xffffffffu, hits, off);
+        exact += __shfl_down_sync(0xffffffffu, exact, off);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd((unsigned long long *)&stats[HTC_STAT_SAMPLES], (unsigned long long)samples);
         atomicAdd((unsigned long long *)&stats[HTC_STAT_HOPS], (unsigned long long)hops);
         atomicAdd((unsigned long long *)&stats[HTC_STAT_OBJECT_TESTS], (unsigned long long)(hops * n_objects));
         atomicAdd((unsigned long long *)&stats[HTC_STAT_HITS], (unsigned long long)hits);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_EXACT_TESTS], (unsigned long long)exact);
     }
 }
 
@@ -182,15 +188,16 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
     float4 *s_inv = smem;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 2 * max_objects);
+    float4 *s_bound = smem + 2 * max_objects;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
     StagedScene s;
-    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_shape, s_hdr)) return;
+    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr)) return;
 
     // 128 threads = 32 x 4 pixels: each warp covers 32 consecutive pixels of a row.
     const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
     const uint32_t y = blockIdx.y * 4 + (threadIdx.x >> 5);
     const bool inside = x < W && y < H;
-    uint32_t n_samples = 0, n_hops = 0, n_hits = 0;
+    uint32_t n_samples = 0, n_hops = 0, n_hits = 0, n_exact = 0;
     if (inside) {
         const uint32_t idx = x + W * y;
         float px, py, size;
@@ -203,7 +210,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
         for (uint32_t i = 0; i < hops; ++i) {
             bool hit;
             n_hops += 1;
-            bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit);
+            bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
             n_hits += hit ? 1 : 0;
             if (!go) break;
         }
@@ -213,7 +220,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
         canvas[idx] = c;
         seeds[idx] = rng;
     }
-    flush_stats(stats, n_samples, n_hops, n_hits, s.n);
+    flush_stats(stats, n_samples, n_hops, n_hits, n_exact, s.n);
 }
 
 // ============================================================================ persistent
@@ -228,13 +235,14 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
     float4 *s_inv = smem;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 2 * max_objects);
+    float4 *s_bound = smem + 2 * max_objects;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
     StagedScene s;
-    const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_shape, s_hdr);
+    const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr);
 
     const uint32_t total = W * H;
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t n_samples = 0, n_hops = 0, n_hits = 0;
+    uint32_t n_samples = 0, n_hops = 0, n_hits = 0, n_exact = 0;
 
     if (staged) {
         uint32_t pixel = NO_PIXEL;
@@ -286,7 +294,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
             if (in_path) {
                 bool hit;
                 n_hops += 1;
-                bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit);
+                bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
                 n_hits += hit ? 1 : 0;
                 hop_i += 1;
                 if (!go || hop_i >= hops) {
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
             }
         }
     }
-    flush_stats(stats, n_samples, n_hops, n_hits, staged ? s.n : 0);
+    flush_stats(stats, n_samples, n_hops, n_hits, n_exact, staged ? s.n : 0);
 
     // The last block to finish rewinds the queue for the next launch.
     __syncthreads();
@@ -380,7 +388,7 @@ static int check_program(const htc_program *p) {
     return HTC_OK;
 }
 static size_t smem_bytes(uint32_t max_objects) {
-    return (size_t)max_objects * 32u + (size_t)max_objects * 4u + 16u;
+    return (size_t)max_objects * 48u + (size_t)max_objects * 4u + 16u;
 }
 static uint32_t objects_capacity(int recipe, size_t scene_size) {
     const size_t hdr = recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;

@@ -47,12 +47,14 @@ extern "C" {
                                   host build (kernel/ocl/random.cc:15-20); the default is
                                   the OpenCL order (first draw -> x). */
 
-/* Render statistics written by the *_ex entry points (device buffer of 4 x uint64,
- * accumulated with atomics; zero it before the launch). */
+/* Render statistics written by the entry points that take a `stats` pointer (device
+ * buffer of HTC_STAT_COUNT x uint64, accumulated with atomics; zero it before the launch). */
 #define HTC_STAT_SAMPLES 0       /* completed paths (scene_sample calls) */
 #define HTC_STAT_HOPS 1          /* executed hop iterations (ray bounces) */
-#define HTC_STAT_OBJECT_TESTS 2  /* object detect calls (hops x objects) */
+#define HTC_STAT_OBJECT_TESTS 2  /* object detect calls the reference makes (hops x objects) */
 #define HTC_STAT_HITS 3          /* hops that hit an object */
+#define HTC_STAT_EXACT_TESTS 4   /* object tests actually evaluated (after distance culling) */
+#define HTC_STAT_COUNT 8
 
 typedef struct htc_program htc_program;
 
@@ -94,7 +96,7 @@ int htc_render(htc_program *program, uint32_t width, uint32_t height, const void
 /* `passes` successive passes in one persistent launch. The result is bit-identical to
  * `passes` htc_render calls: each pixel's samples run in order on one thread, which keeps
  * its RNG stream, and finished paths are regenerated in place so lanes stay busy.
- * stats (optional, device uint64[4]) accumulates the HTC_STAT_* counters. */
+ * stats (optional, device uint64[HTC_STAT_COUNT]) accumulates the HTC_STAT_* counters. */
 int htc_render_passes(htc_program *program, uint32_t width, uint32_t height, const void *scene,
                       size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
                       uint64_t *stats, void *stream);

@@ -157,7 +157,7 @@ def test_render_matches_golden(built, name, persistent):
     seeds = np.zeros(W * H, dtype=np.uint32)
     seeds[pix] = f["seeds_in"]
     seeds_t = torch.from_numpy(seeds.view(np.int32)).to(ctx.device)
-    stats = torch.zeros(4, dtype=torch.int64, device=ctx.device)
+    stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
     r = P.Render(ctx, int(f["recipe"]), int(f["hops"]), _lib.HTC_FLAG_JITTER_YX)
     if persistent:
         _lib.call("htc_render_passes", r.handle, W, H, scene.data_ptr(), scene.numel(), canvas.data_ptr(),
