@@ -330,17 +330,17 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const uint8_t *obj = s.objects + (size_t)kmin * OBJ_STRIDE;
     const Mo fwd = load_mo(obj);
     const bool repeat = (kmin == prev_hash);
-    HyRay l = ray_hy_map(inv, p, v);
+    HyRay l = ray_hy_map_call(inv, p, v);
     HyPath lh;
     Q4 normal;
     if (s.shape[kmin] == 0) plane_hy_hit(l.p, l.v, lh, normal);
     else horosphere_hit(l.p, l.v, repeat, lh, normal);
-    HyRay w = ray_hy_map(fwd, lh.p, lh.v);          // detect: map back (mapped.inl:34)
-    HyRay loc = ray_hy_map(inv, w.p, w.v);          // interact: to local (mapped.inl:46-47)
+    HyRay w = ray_hy_map_call(fwd, lh.p, lh.v);          // detect: map back (mapped.inl:34)
+    HyRay loc = ray_hy_map_call(inv, w.p, w.v);          // interact: to local (mapped.inl:46-47)
     Material m = load_material(obj);
     V3 dir = v3(loc.v.x, loc.v.y, loc.v.z);          // light_hy_to_local (light/hy.cc:3-8)
     bool ret = mixture_interact(m, rng, v3(normal.x, normal.y, normal.z), dir, intensity, emission);
-    HyRay out = ray_hy_map(fwd, loc.p, q4(dir.x, dir.y, dir.z, 0.0f));  // mapped.inl:49
+    HyRay out = ray_hy_map_call(fwd, loc.p, q4(dir.x, dir.y, dir.z, 0.0f));  // mapped.inl:49
     ray.p = out.p;
     ray.v = out.v;
     if (!ret) return false;
