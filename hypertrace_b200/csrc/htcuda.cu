@@ -16,6 +16,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/htcuda.h"
@@ -619,6 +620,102 @@ int htc_extract_gamma_pack(uint32_t W, uint32_t H, uint32_t passes, float gamma,
     uint32_t n = W * H;
     k_extract_gamma_pack<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         n, (float)passes, gamma, reinterpret_cast<const float4 *>(canvas), reinterpret_cast<uchar4 *>(packed));
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+// ---------------------------------------------------------------- allocation-free entry
+// Scratch of htc_render_passes_noalloc: the persistent kernel's work-queue words
+// ([0] next pixel, [1] finished blocks) and a fallback error word ([2]). A file-scope
+// device array, so the entry point never allocates; it lives on every device that loads
+// this library until the process exits. In host code `g_noalloc_scratch` is only a
+// stand-in for the symbol: its device address comes from cudaGetSymbolAddress.
+constexpr uint32_t NOALLOC_SCRATCH_WORDS = 64;   // 256 bytes
+constexpr uint64_t NOALLOC_MAX_PIXELS = 1ull << 31;   // the queue word counts pixels
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+uint32_t *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+int g_noalloc_sms[NOALLOC_MAX_DEVICES];
+int g_noalloc_smem[NOALLOC_MAX_DEVICES];
+
+// Once per device, with that device current: resolve the scratch address and the launch
+// limits. Allocates nothing.
+int noalloc_setup(int dev, uint32_t **scratch, int *num_sms, int *max_smem) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(HTC_ERR_UNSUPPORTED, "device index beyond the supported range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        uint32_t *ptr = nullptr;
+        HTC_CUDA(cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), g_noalloc_scratch));
+        int sms = 0, smem = 0;
+        HTC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        HTC_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        smem -= 1024;
+        int rc = set_smem_attr<RECIPE_HY>(smem);
+        if (rc) return rc;
+        rc = set_smem_attr<RECIPE_EU>(smem);
+        if (rc) return rc;
+        g_noalloc_sms[dev] = sms;
+        g_noalloc_smem[dev] = smem;
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *scratch = g_noalloc_ptr[dev];
+    *num_sms = g_noalloc_sms[dev];
+    *max_smem = g_noalloc_smem[dev];
+    return HTC_OK;
+}
+}  // namespace
+
+int htc_render_passes_noalloc(int recipe, uint32_t light_hops, int address_width, uint32_t flags, uint32_t W,
+                              uint32_t H, const void *scene, size_t scene_size, float *canvas, uint32_t *seeds,
+                              uint32_t passes, uint64_t *stats, uint32_t *status, void *stream) {
+    if (recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU) return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
+    if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
+    if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
+    if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    if (W == 0 || H == 0) return fail(HTC_ERR_INVALID, "canvas width and height must be positive");
+    if ((uint64_t)W * (uint64_t)H > NOALLOC_MAX_PIXELS)
+        return fail(HTC_ERR_UNSUPPORTED, "htc_render_passes_noalloc serves at most 2^31 pixels per call (width*height)");
+    if (!scene || !canvas || !seeds) return fail(HTC_ERR_INVALID, "scene, canvas and seeds must be device pointers");
+    if ((reinterpret_cast<uintptr_t>(scene) & 15u) != 0 || (reinterpret_cast<uintptr_t>(canvas) & 15u) != 0)
+        return fail(HTC_ERR_INVALID, "scene and canvas must be 16-byte aligned");
+    if (scene_size < (recipe == HTC_RECIPE_HY ? 128u : 80u))
+        return fail(HTC_ERR_SCENE, "scene buffer is smaller than the scene header");
+    int dev = 0;
+    HTC_CUDA(cudaGetDevice(&dev));
+    uint32_t *scratch = nullptr;
+    int num_sms = 0, max_smem = 0;
+    int rc = noalloc_setup(dev, &scratch, &num_sms, &max_smem);
+    if (rc) return rc;
+    const uint32_t max_objects = objects_capacity(recipe, scene_size);
+    const size_t smem = smem_bytes(max_objects);
+    if (smem > (size_t)max_smem) return fail(HTC_ERR_UNSUPPORTED, "scene has more objects than shared memory can stage");
+    if (passes == 0) return HTC_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // The queue words must start at zero; the array keeps whatever the last call left.
+    HTC_CUDA(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), st));
+    int per_sm = 0;
+    cudaError_t e = recipe == HTC_RECIPE_HY
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent<RECIPE_HY>, 128, smem)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent<RECIPE_EU>, 128, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)num_sms;
+    const uint64_t needed = ((uint64_t)W * H + 127) / 128;
+    if (blocks > needed) blocks = needed;
+    uint32_t *err = status ? status : scratch + 2;
+    const uint8_t *sc = reinterpret_cast<const uint8_t *>(scene);
+    float4 *cv = reinterpret_cast<float4 *>(canvas);
+    if (recipe == HTC_RECIPE_HY)
+        render_persistent<RECIPE_HY><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, address_width, W, H,
+                                                                          light_hops, passes, flags, cv, seeds, stats, err,
+                                                                          scratch);
+    else
+        render_persistent<RECIPE_EU><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, address_width, W, H,
+                                                                          light_hops, passes, flags, cv, seeds, stats, err,
+                                                                          scratch);
     HTC_CUDA(cudaGetLastError());
     return HTC_OK;
 }

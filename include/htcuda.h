@@ -101,6 +101,23 @@ int htc_render_passes(htc_program *program, uint32_t width, uint32_t height, con
                       size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
                       uint64_t *stats, void *stream);
 
+/* Allocation-free form of htc_render_passes, for callers that cannot call cudaMalloc --
+ * e.g. hosts that hand the renderer a fixed memory budget, or custom allocators that own
+ * all device memory -- and so cannot create an htc_program (which allocates its queue and
+ * error words). No counterpart in the reference. The recipe, hop count, address width and
+ * flags are passed directly; the work-queue words live in a 256-byte file-scope device array
+ * that every device loading the library holds until exit. The first call on a device
+ * resolves that array's address (cudaGetSymbolAddress) and the launch limits, so make the
+ * first call on each device before any stream capture. Calls share the array and zero it
+ * on entry: calls that overlap on the GPU race and must not be issued concurrently.
+ * Limit: width*height <= 2^31 pixels (HTC_ERR_UNSUPPORTED beyond). `status` (optional,
+ * device uint32, zeroed by the caller) receives the scene-validation error bits that
+ * htc_program_check would report (non-zero = HTC_ERR_SCENE). */
+int htc_render_passes_noalloc(int recipe, uint32_t light_hops, int address_width, uint32_t flags,
+                              uint32_t width, uint32_t height, const void *scene, size_t scene_size,
+                              float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats,
+                              uint32_t *status, void *stream);
+
 /* htc_render with statistics (the plain one-pass kernel). */
 int htc_render_ex(htc_program *program, uint32_t width, uint32_t height, const void *scene,
                   size_t scene_size, float *canvas, uint32_t *seeds, uint64_t *stats,
