@@ -55,7 +55,22 @@ SIGNATURES = [
     ("htc_pack", _i, [_u32, _u32, _vp, _vp, _vp]),
     ("htc_extract_gamma_pack", _i, [_u32, _u32, _u32, _f, _vp, _vp, _vp]),
     ("htc_fp32_probe", _i, [_vp, _u32, _i, ctypes.POINTER(ctypes.c_double), _vp]),
+    ("htc_batch_create", _i, [_u32, _u32, ctypes.POINTER(_vp)]),
+    ("htc_batch_destroy", None, [_vp]),
+    ("htc_batch_set_views", _i, [_vp, _vp, _u32, _u32, _u32, _vp]),
+    ("htc_batch_render", _i, [_vp, _vp, _vp]),
+    ("htc_batch_graph_launch", _i, [_vp, _vp, _vp]),
+    ("htc_batch_check", _i, [_vp, _vp]),
+    ("htc_batch_tile_count", _i, [_vp, ctypes.POINTER(_u32)]),
 ]
+
+
+class HtcView(ctypes.Structure):
+    """struct htc_view (include/htcuda.h)."""
+    _fields_ = [("scene", ctypes.c_void_p), ("scene_size", ctypes.c_uint64), ("canvas", ctypes.c_void_p),
+                ("seeds", ctypes.c_void_p), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("recipe", ctypes.c_int32), ("light_hops", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("address_width", ctypes.c_int32), ("passes", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class HtcError(RuntimeError):

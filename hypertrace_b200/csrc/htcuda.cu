@@ -14,10 +14,13 @@
 // memory once per block; the object scan reads them as warp-uniform broadcasts.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/htcuda.h"
 #include "ht_trace.cuh"
@@ -227,6 +230,99 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
 // ============================================================================ persistent
 constexpr uint32_t NO_PIXEL = 0xFFFFFFFFu;
 
+// Counters of one thread, flushed once per launch.
+struct LaneStats {
+    uint32_t samples = 0, hops = 0, hits = 0, exact = 0;
+};
+
+// The persistent lane loop shared by render_persistent and render_batch: warps take pixel
+// indices [first, first + count) from `*counter` (global or shared memory) with one atomic
+// per warp; each lane renders its pixel's `passes` samples in order and regenerates a camera
+// ray as soon as a path ends. Returns when the warp has no pixel left.
+template <int R>
+__device__ __forceinline__ void trace_pixels(const StagedScene &s, uint32_t *counter, uint32_t first,
+                                             uint32_t count, uint32_t W, uint32_t H, uint32_t hops,
+                                             uint32_t passes, uint32_t flags, float4 *__restrict__ canvas,
+                                             uint32_t *__restrict__ seeds, LaneStats &st) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t pixel = NO_PIXEL;
+    bool done = passes == 0;
+    uint32_t pass = 0, rng = 0, prev_hash = HASH_NEVER, hop_i = 0;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    float px = 0.f, py = 0.f, size = 0.f;
+    typename PathOf<R>::T ray;
+    Col intensity = {1.0f, 1.0f, 1.0f};
+    Col emission = {0.0f, 0.0f, 0.0f};
+    bool in_path = false;
+
+    for (;;) {
+        // Lanes without a pixel take the next ones from the counter: one atomic per warp.
+        const bool need = !done && pixel == NO_PIXEL;
+        const uint32_t mask = __ballot_sync(0xffffffffu, need);
+        if (mask) {
+            uint32_t base = 0;
+            const int leader = __ffs(mask) - 1;
+            if (lane == (uint32_t)leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const uint32_t mine = base + __popc(mask & ((1u << lane) - 1u));
+                if (mine < count) {
+                    pixel = first + mine;
+                    const uint32_t x = pixel % W, y = pixel / W;
+                    pixel_pos(x, y, W, H, px, py, size);
+                    rng = seeds[pixel];
+                    acc = canvas[pixel];
+                    pass = 0;
+                    in_path = false;
+                } else {
+                    done = true;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        if (pixel != NO_PIXEL && !in_path) {
+            ray = camera<R>(s, px, py, size, rng, flags);
+            intensity.x = intensity.y = intensity.z = 1.0f;
+            emission.x = emission.y = emission.z = 0.0f;
+            prev_hash = HASH_NEVER;
+            hop_i = 0;
+            in_path = true;
+        }
+        if (in_path) {
+            bool hit;
+            st.hops += 1;
+            bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact);
+            st.hits += hit ? 1 : 0;
+            hop_i += 1;
+            if (!go || hop_i >= hops) {
+                acc.x += emission.x; acc.y += emission.y; acc.z += emission.z; acc.w += 1.0f;
+                st.samples += 1;
+                in_path = false;
+                pass += 1;
+                if (pass >= passes) {
+                    canvas[pixel] = acc;
+                    seeds[pixel] = rng;
+                    pixel = NO_PIXEL;
+                }
+            }
+        }
+    }
+}
+
+// The last block to finish rewinds the launch's queue words for the next launch.
+__device__ __forceinline__ void rewind_queue(uint32_t *queue) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t finished = atomicAdd(&queue[1], 1u);
+        if (finished == gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 template <int R>
 __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
@@ -240,91 +336,104 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
     StagedScene s;
     const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr);
+    LaneStats st;
+    if (staged) trace_pixels<R>(s, &queue[0], 0, W * H, W, H, hops, passes, flags, canvas, seeds, st);
+    flush_stats(stats, st.samples, st.hops, st.hits, st.exact, staged ? s.n : 0);
+    rewind_queue(queue);
+}
 
-    const uint32_t total = W * H;
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t n_samples = 0, n_hops = 0, n_hits = 0, n_exact = 0;
+// ============================================================================ batch
+// Many views (scenes, resolutions, pass counts, either recipe) in one persistent launch.
+// Blocks take tiles (view, pixel range) from a global queue; a block stages a view's scene
+// in shared memory only when its tile's view differs from the one it holds; the block's
+// warps then pull the tile's pixels from a shared-memory counter. Per-pixel sample order is
+// the same as in render_persistent, so every view's result is bit-identical to rendering it
+// alone.
+struct BatchView {          // device copy of htc_view plus host-derived fields
+    const uint8_t *scene;
+    uint64_t scene_size;
+    float4 *canvas;
+    uint32_t *seeds;
+    uint32_t width, height;
+    int32_t recipe;
+    uint32_t hops, flags;
+    int32_t address_width;
+    uint32_t passes;
+    uint32_t max_objects;   // objects the scene buffer can hold
+};
+struct BatchTile { uint32_t view, first, count; };
 
-    if (staged) {
-        uint32_t pixel = NO_PIXEL;
-        bool done = false;
-        uint32_t pass = 0, rng = 0, prev_hash = HASH_NEVER, hop_i = 0;
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        float px = 0.f, py = 0.f, size = 0.f;
-        typename PathOf<R>::T ray;
-        Col intensity = {1.0f, 1.0f, 1.0f};
-        Col emission = {0.0f, 0.0f, 0.0f};
-        bool in_path = false;
-
-        for (;;) {
-            // Lanes without a pixel take the next ones from the queue: one atomic per warp.
-            const bool need = !done && pixel == NO_PIXEL;
-            const uint32_t mask = __ballot_sync(0xffffffffu, need);
-            if (mask) {
-                uint32_t base = 0;
-                const int leader = __ffs(mask) - 1;
-                if (lane == (uint32_t)leader) base = atomicAdd(&queue[0], (uint32_t)__popc(mask));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (need) {
-                    const uint32_t mine = base + __popc(mask & ((1u << lane) - 1u));
-                    if (mine < total) {
-                        pixel = mine;
-                        const uint32_t x = pixel % W, y = pixel / W;
-                        pixel_pos(x, y, W, H, px, py, size);
-                        rng = seeds[pixel];
-                        acc = canvas[pixel];
-                        pass = 0;
-                        in_path = false;
-                        if (passes == 0) {   // nothing to render: leave the pixel as it is
-                            pixel = NO_PIXEL;
-                        }
-                    } else {
-                        done = true;
-                    }
-                }
+__global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
+    const BatchView *__restrict__ views, const BatchTile *__restrict__ tiles, uint32_t n_tiles,
+    uint32_t smem_objects, uint64_t *stats, uint32_t *err, uint32_t *queue) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_tile, s_next;
+    __shared__ int s_staged_view, s_staged_ok;
+    float4 *s_inv = smem;
+    float4 *s_bound = smem + 2 * smem_objects;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * smem_objects);
+    StagedScene s;
+    s.n = 0;
+    LaneStats st;
+    uint64_t object_tests = 0;
+    if (threadIdx.x == 0) s_staged_view = -1;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_tile = atomicAdd(&queue[0], 1u);
+            s_next = 0;
+        }
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t >= n_tiles) break;
+        const BatchTile tile = tiles[t];
+        const BatchView &v = views[tile.view];
+        const int32_t recipe = v.recipe;
+        if ((int)tile.view != s_staged_view) {
+            bool ok;
+            if (recipe == RECIPE_HY)
+                ok = stage_scene<RECIPE_HY>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
+                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+            else
+                ok = stage_scene<RECIPE_EU>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
+                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_staged_view = (int)tile.view;
+                s_staged_ok = ok ? 1 : 0;
             }
-            if (__all_sync(0xffffffffu, done)) break;
-            if (pixel != NO_PIXEL && !in_path) {
-                ray = camera<R>(s, px, py, size, rng, flags);
-                intensity.x = intensity.y = intensity.z = 1.0f;
-                emission.x = emission.y = emission.z = 0.0f;
-                prev_hash = HASH_NEVER;
-                hop_i = 0;
-                in_path = true;
-            }
-            if (in_path) {
-                bool hit;
-                n_hops += 1;
-                bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
-                n_hits += hit ? 1 : 0;
-                hop_i += 1;
-                if (!go || hop_i >= hops) {
-                    acc.x += emission.x; acc.y += emission.y; acc.z += emission.z; acc.w += 1.0f;
-                    n_samples += 1;
-                    in_path = false;
-                    pass += 1;
-                    if (pass >= passes) {
-                        canvas[pixel] = acc;
-                        seeds[pixel] = rng;
-                        pixel = NO_PIXEL;
-                    }
-                }
-            }
+            __syncthreads();
+        }
+        // (every thread staged the current view, so its StagedScene `s` still describes it)
+        if (!s_staged_ok) continue;
+        const uint32_t hops_before = st.hops;
+        if (recipe == RECIPE_HY)
+            trace_pixels<RECIPE_HY>(s, &s_next, tile.first, tile.count, v.width, v.height, v.hops, v.passes, v.flags,
+                                    v.canvas, v.seeds, st);
+        else
+            trace_pixels<RECIPE_EU>(s, &s_next, tile.first, tile.count, v.width, v.height, v.hops, v.passes, v.flags,
+                                    v.canvas, v.seeds, st);
+        object_tests += (uint64_t)(st.hops - hops_before) * s.n;
+    }
+    if (stats) {
+        uint64_t samples = st.samples, hops = st.hops, hits = st.hits, exact = st.exact, tests = object_tests;
+        for (int off = 16; off > 0; off >>= 1) {
+            samples += __shfl_down_sync(0xffffffffu, samples, off);
+            hops += __shfl_down_sync(0xffffffffu, hops, off);
+            hits += __shfl_down_sync(0xffffffffu, hits, off);
+            exact += __shfl_down_sync(0xffffffffu, exact, off);
+            tests += __shfl_down_sync(0xffffffffu, tests, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd((unsigned long long *)&stats[HTC_STAT_SAMPLES], (unsigned long long)samples);
+            atomicAdd((unsigned long long *)&stats[HTC_STAT_HOPS], (unsigned long long)hops);
+            atomicAdd((unsigned long long *)&stats[HTC_STAT_OBJECT_TESTS], (unsigned long long)tests);
+            atomicAdd((unsigned long long *)&stats[HTC_STAT_HITS], (unsigned long long)hits);
+            atomicAdd((unsigned long long *)&stats[HTC_STAT_EXACT_TESTS], (unsigned long long)exact);
         }
     }
-    flush_stats(stats, n_samples, n_hops, n_hits, n_exact, staged ? s.n : 0);
-
-    // The last block to finish rewinds the queue for the next launch.
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const uint32_t finished = atomicAdd(&queue[1], 1u);
-        if (finished == gridDim.x - 1) {
-            queue[0] = 0;
-            queue[1] = 0;
-            __threadfence();
-        }
-    }
+    rewind_queue(queue);
 }
 
 // ============================================================================ post
@@ -621,6 +730,197 @@ int htc_extract_gamma_pack(uint32_t W, uint32_t H, uint32_t passes, float gamma,
     k_extract_gamma_pack<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         n, (float)passes, gamma, reinterpret_cast<const float4 *>(canvas), reinterpret_cast<uchar4 *>(packed));
     HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+// ---------------------------------------------------------------- batches
+}  // extern "C"
+
+struct htc_batch {
+    uint32_t max_views, max_tiles;
+    BatchView *d_views;
+    BatchTile *d_tiles;
+    uint32_t *d_queue;   // [0] next tile, [1] finished blocks
+    uint32_t *d_err;
+    uint32_t n_tiles;
+    uint32_t smem_objects;
+    uint32_t blocks_per_sm;
+    int num_sms, max_smem;
+    cudaGraph_t graph;
+    cudaGraphExec_t graph_exec;
+    std::vector<BatchView> h_views;
+    std::vector<BatchTile> h_tiles;
+};
+
+static void batch_free(htc_batch *b) {
+    if (!b) return;
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_views);
+    cudaFree(b->d_tiles);
+    cudaFree(b->d_queue);
+    cudaFree(b->d_err);
+    delete b;
+}
+
+static int batch_launch(htc_batch *b, uint64_t *stats, cudaStream_t st) {
+    if (b->n_tiles == 0) return HTC_OK;
+    const size_t smem = smem_bytes(b->smem_objects);
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch, 128, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)b->num_sms;
+    if (blocks > b->n_tiles) blocks = b->n_tiles;
+    render_batch<<<(unsigned)blocks, 128, smem, st>>>(b->d_views, b->d_tiles, b->n_tiles, b->smem_objects, stats,
+                                                      b->d_err, b->d_queue);
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
+extern "C" {
+
+int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
+    if (!out) return fail(HTC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (max_views == 0 || max_tiles == 0) return fail(HTC_ERR_INVALID, "max_views and max_tiles must be positive");
+    int dev = 0;
+    HTC_CUDA(cudaGetDevice(&dev));
+    htc_batch *b = new htc_batch();
+    b->max_views = max_views;
+    b->max_tiles = max_tiles;
+    cudaError_t e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_views, sizeof(BatchView) * max_views);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * max_tiles);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) {
+        b->max_smem -= 1024;
+        e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+    }
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return cuda_fail(e, "htc_batch_create");
+    }
+    *out = b;
+    return HTC_OK;
+}
+
+void htc_batch_destroy(htc_batch *b) { batch_free(b); }
+
+int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, uint32_t tile_pixels,
+                        uint32_t blocks_per_sm, void *stream) {
+    if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
+    if (n_views > b->max_views) return fail(HTC_ERR_INVALID, "more views than the batch was created for");
+    if (n_views && !views) return fail(HTC_ERR_INVALID, "views is NULL");
+    if (tile_pixels == 0) return fail(HTC_ERR_INVALID, "tile_pixels must be positive");
+    b->h_views.assign(n_views, BatchView());
+    b->h_tiles.clear();
+    uint32_t smem_objects = 0;
+    std::vector<std::pair<double, uint32_t>> order;
+    for (uint32_t i = 0; i < n_views; ++i) {
+        const htc_view &v = views[i];
+        if (v.recipe != HTC_RECIPE_HY && v.recipe != HTC_RECIPE_EU) return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe in a view");
+        if (v.light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
+        if (v.address_width != 32 && v.address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
+        if (v.flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown view flags");
+        if (v.width == 0 || v.height == 0 || (uint64_t)v.width * v.height >= 0xFFFFFFFFull)
+            return fail(HTC_ERR_INVALID, "view size must be positive and fit 32 bits");
+        if (!v.scene || !v.canvas || !v.seeds) return fail(HTC_ERR_INVALID, "view buffers must be device pointers");
+        if ((reinterpret_cast<uintptr_t>(v.scene) & 15u) || (reinterpret_cast<uintptr_t>(v.canvas) & 15u))
+            return fail(HTC_ERR_INVALID, "scene and canvas must be 16-byte aligned");
+        if (v.scene_size < (v.recipe == HTC_RECIPE_HY ? 128u : 80u)) return fail(HTC_ERR_SCENE, "view scene smaller than its header");
+        BatchView &d = b->h_views[i];
+        d.scene = reinterpret_cast<const uint8_t *>(v.scene);
+        d.scene_size = v.scene_size;
+        d.canvas = reinterpret_cast<float4 *>(v.canvas);
+        d.seeds = v.seeds;
+        d.width = v.width;
+        d.height = v.height;
+        d.recipe = v.recipe;
+        d.hops = v.light_hops;
+        d.flags = v.flags;
+        d.address_width = v.address_width;
+        d.passes = v.passes;
+        d.max_objects = objects_capacity(v.recipe, v.scene_size);
+        if (v.passes == 0) continue;
+        if (d.max_objects > smem_objects) smem_objects = d.max_objects;
+        // cost per pixel ~ passes x hops x objects: expensive views first (longest-first order
+        // shortens the tail of the persistent launch)
+        order.push_back({(double)v.passes * v.light_hops * (1.0 + d.max_objects), i});
+    }
+    if (smem_bytes(smem_objects) > (size_t)b->max_smem)
+        return fail(HTC_ERR_UNSUPPORTED, "a view has more objects than shared memory can stage");
+    std::stable_sort(order.begin(), order.end(), [](const std::pair<double, uint32_t> &a, const std::pair<double, uint32_t> &c) { return a.first > c.first; });
+    for (const auto &o : order) {
+        const BatchView &d = b->h_views[o.second];
+        const uint32_t total = d.width * d.height;
+        for (uint32_t first = 0; first < total; first += tile_pixels) {
+            if (b->h_tiles.size() >= b->max_tiles) return fail(HTC_ERR_INVALID, "more tiles than the batch was created for (raise max_tiles or tile_pixels)");
+            b->h_tiles.push_back({o.second, first, std::min(tile_pixels, total - first)});
+        }
+    }
+    b->n_tiles = (uint32_t)b->h_tiles.size();
+    b->smem_objects = smem_objects;
+    b->blocks_per_sm = blocks_per_sm;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->h_views.data(), sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
+    if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));
+    HTC_CUDA(cudaStreamSynchronize(st));   // the host vectors are reused by the next call
+    if (b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    return HTC_OK;
+}
+
+int htc_batch_render(htc_batch *b, uint64_t *stats, void *stream) {
+    if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
+    return batch_launch(b, stats, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int htc_batch_graph_launch(htc_batch *b, uint64_t *stats, void *stream) {
+    if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (!b->graph_exec) {
+        cudaStream_t cap;
+        HTC_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        int rc = HTC_OK;
+        if (e == cudaSuccess) rc = batch_launch(b, stats, cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->graph_exec, g, 0);
+        if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "cudaGraphInstantiate"); }
+        b->graph = g;
+    }
+    HTC_CUDA(cudaGraphLaunch(b->graph_exec, st));
+    return HTC_OK;
+}
+
+int htc_batch_check(htc_batch *b, void *stream) {
+    if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
+    uint32_t err = 0;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    HTC_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    HTC_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        HTC_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), st));
+        HTC_CUDA(cudaStreamSynchronize(st));
+        return fail(HTC_ERR_SCENE, "a view's scene bytes failed validation");
+    }
+    return HTC_OK;
+}
+
+int htc_batch_tile_count(const htc_batch *b, uint32_t *n_tiles) {
+    if (!b || !n_tiles) return fail(HTC_ERR_INVALID, "batch or n_tiles is NULL");
+    *n_tiles = b->n_tiles;
     return HTC_OK;
 }
 

@@ -123,6 +123,41 @@ int htc_render_ex(htc_program *program, uint32_t width, uint32_t height, const v
                   size_t scene_size, float *canvas, uint32_t *seeds, uint64_t *stats,
                   void *stream);
 
+/* ---------------------------------------------------------------- batches
+ * Many views -- scenes of either recipe, resolutions, hop counts and pass counts -- in one
+ * persistent launch (no counterpart in the reference, whose Pipeline renders one view per
+ * enqueue). Each view's result is bit-identical to rendering it alone with
+ * htc_render_passes: pixels keep their own RNG streams and sample order. */
+typedef struct htc_view {
+    const void *scene;       /* device pointer to the serialized scene bytes */
+    uint64_t scene_size;
+    float *canvas;           /* device float4[width*height], accumulated */
+    uint32_t *seeds;         /* device uint32[width*height], advanced in place */
+    uint32_t width, height;
+    int32_t recipe;          /* HTC_RECIPE_* */
+    uint32_t light_hops;
+    uint32_t flags;          /* HTC_FLAG_* */
+    int32_t address_width;   /* 32 or 64 */
+    uint32_t passes;         /* passes of this view rendered by each launch (0 = skip) */
+    uint32_t reserved;
+} htc_view;
+
+typedef struct htc_batch htc_batch;
+int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out);
+void htc_batch_destroy(htc_batch *batch);
+/* Uploads the views and cuts them into tiles of `tile_pixels` pixels (most expensive views
+ * first); blocks_per_sm caps residency (0 = as many as fit). Synchronises `stream`. */
+int htc_batch_set_views(htc_batch *batch, const htc_view *views, uint32_t n_views,
+                        uint32_t tile_pixels, uint32_t blocks_per_sm, void *stream);
+/* One launch rendering every view's `passes`. stats as in htc_render_passes. */
+int htc_batch_render(htc_batch *batch, uint64_t *stats, void *stream);
+/* The same launch through a CUDA graph captured on first use (re-captured after
+ * htc_batch_set_views); `stats` is baked into the graph at capture. */
+int htc_batch_graph_launch(htc_batch *batch, uint64_t *stats, void *stream);
+/* Reads and clears the batch's device error word (synchronises `stream`). */
+int htc_batch_check(htc_batch *batch, void *stream);
+int htc_batch_tile_count(const htc_batch *batch, uint32_t *n_tiles);
+
 /* ---------------------------------------------------------------- post chain
  * Extractor (processing/src/canvas.rs:126-135): image = canvas / passes.
  * GammaFilter (processing/src/filter/gamma.rs:10-19): out = pow(max(in, 0), gamma).

@@ -1,0 +1,74 @@
+"""Batched launches: every view's result equals rendering it alone (bit for bit), for a
+mix of recipes, sizes and pass counts, directly and through the captured CUDA graph."""
+import numpy as np
+import pytest
+import torch
+
+from hypertrace_b200 import batch as B
+from hypertrace_b200 import processing as P
+from hypertrace_b200 import scene as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _views(seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i, (w, h) in enumerate([(64, 48), (37, 29), (128, 72), (16, 16), (96, 40), (50, 50)]):
+        if i % 2 == 0:
+            sc = S.euclidean_scene(int(rng.integers(2, 9)), 4, 100 + i, camera=B.random_hom3(rng))
+        else:
+            sc = S.hyperbolic_scene(int(rng.integers(2, 30)), int(rng.integers(2, 40)), 5.0, 8, 200 + i,
+                                    camera=S.random_moebius(rng, 1.0))
+        out.append(B.View(sc, w, h, 4, 1000 + i))
+    return out
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("tile", [64, 1000])
+def test_batch_equals_alone(built, graph, tile):
+    ctx = P.Context(0)
+    views = _views()
+    alone = _views()
+    for v in views + alone:
+        v.allocate(ctx)
+    passes = [1, 3, 2, 4, 1, 2]
+    br = B.BatchRenderer(ctx, max_views=16, max_tiles=4096)
+    br.set_views(views, passes, tile_pixels=tile, blocks_per_sm=0)
+    for _ in range(2):
+        br.render(graph=graph)
+    br.check()
+    for v, p in zip(alone, passes):
+        r = P.Render(ctx, v.scene.recipe, v.scene.hops)
+        r.render_passes(v.buffer, v.canvas, 2 * p)
+    torch.cuda.synchronize()
+    for a, b in zip(views, alone):
+        assert torch.equal(a.canvas.seeds, b.canvas.seeds)
+        assert np.array_equal(a.canvas.image.cpu().numpy().view(np.uint32), b.canvas.image.cpu().numpy().view(np.uint32))
+
+
+def test_batch_zero_pass_view_untouched(built):
+    ctx = P.Context(0)
+    views = _views()[:3]
+    for v in views:
+        v.allocate(ctx)
+    before = views[1].canvas.image.clone()
+    br = B.BatchRenderer(ctx, max_views=4, max_tiles=1024)
+    br.set_views(views, [1, 0, 1], tile_pixels=256)
+    br.render()
+    br.check()
+    torch.cuda.synchronize()
+    assert torch.equal(before, views[1].canvas.image)
+
+
+def test_batch_autotune_restores_state(built):
+    ctx = P.Context(0)
+    views = _views()
+    for v in views:
+        v.allocate(ctx)
+    snap = [v.canvas.seeds.clone() for v in views]
+    br = B.BatchRenderer(ctx, max_views=16, max_tiles=4096)
+    tile, res, t = B.autotune(br, views, tiles=(128, 1024), residency=(4, 6))
+    assert (tile, res) in t and len(t) == 4
+    for v, s in zip(views, snap):
+        assert torch.equal(v.canvas.seeds, s)
