@@ -47,6 +47,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--passes", type=int, default=4, help="passes (samples per pixel) per step")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["hy1080", "batched", "serving"], default="hy1080",
+                    help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views in one "
+                         "launch per step; serving: Poisson requests through the continuous-batching server")
+    ap.add_argument("--spp-scale", type=float, default=0.25, help="batched: scale of every view's spp")
+    ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
+    ap.add_argument("--rates", type=str, default="50,200,1000,2000", help="serving: arrival rates (req/s)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -198,6 +204,10 @@ def main():
 
     hb.build()
     torch.cuda.set_device(local_rank)
+    if args.workload == "batched":
+        return bench_batched(args)
+    if args.workload == "serving":
+        return bench_serving(args)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -360,6 +370,108 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _time_ms(fn, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def bench_batched(args):
+    """The mixed workload (96 views: resolutions from {256^2, 640x480, 1280x720, 1920x1080},
+    spp in {16..256} x --spp-scale, half Euclidean / half hyperbolic with 20-200 objects):
+    batched persistent launches (autotuned tile size / residency, CUDA graphs, 16 passes of
+    every unfinished view per step) against the same views rendered one at a time with the
+    plain one-pass kernel and with the single-view persistent kernel. Results of the three
+    are bit-identical (tests/test_gpu_batch.py), so RMSE against any reference is equal."""
+    import torch
+    from hypertrace_b200 import batch as B
+    from hypertrace_b200 import processing as P
+    ctx = P.Context(0)
+    stream = torch.cuda.current_stream(ctx.device)
+    views = B.config3(spp_scale=args.spp_scale)
+    for v in views:
+        v.allocate(ctx)
+    total_samples = sum(v.width * v.height * v.spp for v in views)
+    br = B.BatchRenderer(ctx, max_views=128, max_tiles=1 << 20)
+    tile, res, timings = B.autotune(br, views)
+    stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+    dev_ms, steps, launches = 0.0, 0, 0
+    active_key = None
+    while any(v.remaining for v in views):
+        active = [v for v in views if v.remaining]
+        passes = [min(16, v.remaining) for v in active]
+        key = (tuple(id(v) for v in active), tuple(passes))
+        if key != active_key:
+            br.set_views(active, passes, tile_pixels=tile, blocks_per_sm=res)
+            active_key = key
+        dev_ms += _time_ms(lambda: br.render(stats=stats, graph=True), stream)
+        for v, p in zip(active, passes):
+            v.done_passes += p
+        steps += 1
+    br.check()
+    st = stats.cpu().numpy().astype(np.float64)
+    batched = {"value": st[0] / dev_ms / 1e3, "unit": UNIT, "device_ms": dev_ms, "steps": steps,
+               "ray_bounces_per_s": st[1] / dev_ms * 1e3, "tile_pixels": tile, "blocks_per_sm": res,
+               "autotune_ms": {f"{k[0]}x{k[1]}": round(t, 3) for k, t in timings.items()}}
+    for v in views:
+        v.release()
+
+    def per_view(persistent):
+        vs = B.config3(spp_scale=args.spp_scale)
+        ms = 0.0
+        renders = {}
+        for v in vs:
+            v.allocate(ctx)
+            key = (v.scene.recipe, v.scene.hops)
+            r = renders.setdefault(key, P.Render(ctx, *key))
+            if persistent:
+                ms += _time_ms(lambda: r.render_passes(v.buffer, v.canvas, v.spp, sync=False), stream)
+            else:
+                ms += _time_ms(lambda: [r.render(v.buffer, v.canvas, sync=False) for _ in range(v.spp)], stream)
+            v.release()
+        return {"value": total_samples / ms / 1e3, "unit": UNIT, "device_ms": ms}
+
+    plain = per_view(False)
+    single = per_view(True)
+    line = {"metric": "Msamples/s, mixed batched workload (96 views, 1 launch per step)", "value": batched["value"],
+            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "mixed-96-views", "spp_scale": args.spp_scale, "total_samples": total_samples,
+                       "passes_per_step": 16},
+            "batched": batched, "plain_per_view": plain, "persistent_per_view": single,
+            "speedup_vs_plain": batched["value"] / plain["value"]}
+    print(json.dumps(line), flush=True)
+
+
+def bench_serving(args):
+    """Poisson arrivals (70 % interactive 1280x720 8-spp frames with a moving camera, 30 %
+    batch jobs drawn from the mixed workload), served by continuous batching under a 120 GB
+    budget, against one-request-at-a-time plain kernels; p50/p99 latency per class."""
+    import torch
+    from hypertrace_b200 import processing as P
+    from hypertrace_b200 import serve as V
+    ctx = P.Context(0)
+    # warm-up: compile-free, but the first launches load modules and size caches
+    V.Server(ctx).run(V.make_requests(6, 1000.0, seed=1))
+    out = {}
+    for rate in [float(x) for x in args.rates.split(",")]:
+        served = V.Server(ctx).run(V.make_requests(args.requests, rate))
+        plain = V.plain_fifo(ctx, V.make_requests(args.requests, rate))
+        out[str(int(rate))] = {"served": served, "plain_fifo": plain}
+        torch.cuda.synchronize()
+    first = out[next(iter(out))]
+    line = {"metric": "serving: throughput and p50/p99 frame latency, continuous batching vs plain per-request",
+            "value": first["served"]["throughput_msamples_per_s"], "unit": UNIT, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "serving", "requests_per_rate": args.requests, "hbm_budget_gb": 120,
+                       "interactive": "1280x720 x 8 spp hyperbolic, moving camera", "batch_spp_scale": 0.125},
+            "rates": out}
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
