@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--passes", type=int, default=4, help="passes (samples per pixel) per step")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hy1080", "batched", "serving"], default="hy1080",
+    ap.add_argument("--workload", choices=["hy1080", "batched", "serving", "accuracy"], default="hy1080",
                     help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views in one "
                          "launch per step; serving: Poisson requests through the continuous-batching server")
     ap.add_argument("--spp-scale", type=float, default=0.25, help="batched: scale of every view's spp")
@@ -208,6 +208,8 @@ def main():
         return bench_batched(args)
     if args.workload == "serving":
         return bench_serving(args)
+    if args.workload == "accuracy":
+        return bench_accuracy(args)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -472,6 +474,57 @@ def bench_serving(args):
                        "interactive": "1280x720 x 8 spp hyperbolic, moving camera", "batch_spp_scale": 0.125},
             "rates": out}
     print(json.dumps(line), flush=True)
+
+
+def bench_accuracy(args):
+    """Error of the FP32 GPU result against the FP64 CPU oracle (same scene bytes, seeds and
+    passes) per pixel, and RMSE of the FP32 GPU image and of the FP64 image against a converged
+    FP64 image (many more passes), on random pixel subsets of the hyperbolic workloads."""
+    import torch
+    from hypertrace_b200 import processing as P
+    from hypertrace_b200 import scene as S
+    from oracle import oracle
+    ctx = P.Context(0)
+    out = {}
+    cores = os.cpu_count() or 1
+    for name, wl, n_pix, passes, conv_passes in (("hyperbolic-800x600-18obj-h6", S.config1(), 400, 64, 1024),
+                                                 ("hyperbolic-1920x1080-200obj-h8", S.config2(), 200, 64, 512)):
+        sc = wl.scene
+        W, H = wl.width, wl.height
+        buf = P.EntityBuffer(ctx, sc)
+        canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
+        seeds0 = canvas.seeds.cpu().numpy().view(np.uint32).copy()
+        P.Render(ctx, sc.recipe, sc.hops).render_passes(buf, canvas, passes)
+        torch.cuda.synchronize()
+        gpu = canvas.image.cpu().numpy().reshape(-1, 4)
+        rng = np.random.default_rng(11)
+        pix = np.sort(rng.choice(W * H, n_pix, replace=False)).astype(np.uint32)
+        data = sc.to_bytes()
+        f32 = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds0[pix], passes=passes, threads=cores)
+        f64 = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds0[pix], passes=passes, threads=cores,
+                            precision=64)
+        conv_seeds = S.pixel_seeds(wl.global_seed ^ 0xC0FFEE, W * H)[pix]
+        conv = oracle.render(data, sc.recipe, sc.hops, W, H, pix, conv_seeds, passes=conv_passes, threads=cores,
+                             precision=64)
+        g = gpu[pix, :3] / passes
+        c32 = f32.canvas[:, :3] / passes
+        c64 = f64.canvas[:, :3] / passes
+        cc = conv.canvas[:, :3] / conv_passes
+        rel = np.abs(g - c64) / np.maximum(np.abs(c64), 1e-3)
+        same_path = f64.seeds == f32.seeds
+        out[name] = {
+            "pixels": int(n_pix), "passes": passes, "converged_passes": conv_passes,
+            "gpu_vs_cpu_f32_bit_identical_fraction": float(np.mean(np.all(g == c32, axis=1))),
+            "gpu_vs_f64_rel_err": {"mean": float(rel.mean()), "median": float(np.median(rel)),
+                                   "max": float(rel.max())},
+            "gpu_vs_f64_rel_err_on_same_paths": {
+                "fraction_of_pixels": float(same_path.mean()),
+                "max": float(rel[same_path].max()) if same_path.any() else None},
+            "rmse_vs_converged_f64": {"gpu_f32": float(np.sqrt(np.mean((g - cc) ** 2))),
+                                      "cpu_f64": float(np.sqrt(np.mean((c64 - cc) ** 2)))},
+        }
+    print(json.dumps({"metric": "error of the FP32 GPU path vs the FP64 oracle", "data": "synthetic",
+                      "results": out}), flush=True)
 
 
 if __name__ == "__main__":

@@ -750,10 +750,25 @@ struct htc_batch {
     cudaGraphExec_t graph_exec;
     std::vector<BatchView> h_views;
     std::vector<BatchTile> h_tiles;
+    // Two pinned staging slots for the asynchronous descriptor upload; slot i may be
+    // rewritten once its last copy (event staged[i]) has run.
+    BatchView *p_views[2];
+    BatchTile *p_tiles[2];
+    size_t p_tiles_cap[2];
+    cudaEvent_t staged[2];
+    int slot;
 };
 
 static void batch_free(htc_batch *b) {
     if (!b) return;
+    for (int i = 0; i < 2; ++i) {
+        if (b->staged[i]) {
+            cudaEventSynchronize(b->staged[i]);
+            cudaEventDestroy(b->staged[i]);
+        }
+        if (b->p_views[i]) cudaFreeHost(b->p_views[i]);
+        if (b->p_tiles[i]) cudaFreeHost(b->p_tiles[i]);
+    }
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_views);
@@ -798,6 +813,10 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_views[i]), sizeof(BatchView) * max_views, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) {
         b->max_smem -= 1024;
         e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
@@ -868,9 +887,23 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     b->smem_objects = smem_objects;
     b->blocks_per_sm = blocks_per_sm;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->h_views.data(), sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
-    if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));
-    HTC_CUDA(cudaStreamSynchronize(st));   // the host vectors are reused by the next call
+    // Asynchronous upload through the next pinned slot: wait only for that slot's previous
+    // copy, then copy on `stream` (ordered after any launch still reading the device arrays).
+    const int k = b->slot;
+    b->slot ^= 1;
+    HTC_CUDA(cudaEventSynchronize(b->staged[k]));
+    if (b->n_tiles > b->p_tiles_cap[k]) {
+        if (b->p_tiles[k]) HTC_CUDA(cudaFreeHost(b->p_tiles[k]));
+        b->p_tiles[k] = nullptr;
+        const size_t cap = std::max<size_t>(b->n_tiles, 4096);
+        HTC_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&b->p_tiles[k]), sizeof(BatchTile) * cap, cudaHostAllocDefault));
+        b->p_tiles_cap[k] = cap;
+    }
+    if (n_views) std::memcpy(b->p_views[k], b->h_views.data(), sizeof(BatchView) * n_views);
+    if (b->n_tiles) std::memcpy(b->p_tiles[k], b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles);
+    if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->p_views[k], sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
+    if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->p_tiles[k], sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));
+    HTC_CUDA(cudaEventRecord(b->staged[k], st));
     if (b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     return HTC_OK;

@@ -46,8 +46,8 @@ class EntityBuffer:
 
     def __init__(self, context: Context, scene: Scene):
         data = serialize(scene, context.config.address_width)
-        host = torch.frombuffer(bytearray(data), dtype=torch.uint8)
-        self.tensor = host.to(context.device)
+        host = torch.frombuffer(bytearray(data), dtype=torch.uint8).pin_memory()
+        self.tensor = host.to(context.device, non_blocking=True)   # ordered on the current stream
         self.size = len(data)
 
     def ptr(self) -> int:
@@ -63,7 +63,8 @@ class Canvas:
         self.context = context
         self.image = torch.zeros(h * w * 4, dtype=torch.float32, device=context.device)
         seeds = pixel_seeds(global_seed, w * h)
-        self.seeds = torch.from_numpy(seeds.view(np.int32).copy()).to(context.device)
+        host = torch.from_numpy(seeds.view(np.int32).copy()).pin_memory()
+        self.seeds = host.to(context.device, non_blocking=True)   # ordered on the current stream
         self.passes = 0
 
     @property

@@ -18,7 +18,7 @@ from __future__ import annotations
 import collections
 import dataclasses
 import time
-from typing import Callable, Dict, List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -90,39 +90,81 @@ def make_requests(n: int, rate: float, seed: int = 0x5EED0004, interactive_share
 class Server:
     """Continuous batching over the htc_batch launch."""
 
-    def __init__(self, ctx: Context, hbm_budget_bytes: int = 120 << 30, tile_pixels: int = 2048,
-                 blocks_per_sm: int = 0, gamma: float = 1.0 / 2.2):
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 120 << 30, tile_pixels: int = 512,
+                 blocks_per_sm: int = 0, gamma: float = 1.0 / 2.2, step_samples: int = 16_000_000):
         self.ctx = ctx
         self.budget = hbm_budget_bytes
+        self.step_samples = step_samples    # work of one step: bounds the wait of a new arrival
         self.renderer = BatchRenderer(ctx, max_views=4096, max_tiles=1 << 21)
         self.tile_pixels = tile_pixels
         self.blocks_per_sm = blocks_per_sm
         self.gamma = gamma
         self.steps = 0
         self.device_s = 0.0
+        self._step_events = []
 
-    def _finish(self, r: Request, now: float, keep_image: bool) -> None:
+    def _enqueue_finish(self, r: Request, keep_image: bool) -> dict:
+        """Post chain + read-back of a finished request, enqueued on the stream (no wait)."""
         v = r.view
         w, h = v.width, v.height
         packed = torch.empty(w * h * 4, dtype=torch.uint8, device=self.ctx.device)
         _lib.call("htc_extract_gamma_pack", w, h, v.spp, _lib.ctypes.c_float(self.gamma),
                   v.canvas.image.data_ptr(), packed.data_ptr(), self.ctx.stream())
-        img = packed.cpu().numpy()   # synchronising read-back of the finished frame
-        r.finished = time.perf_counter() - now
+        out = {"image": torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)}
+        out["image"].copy_(packed, non_blocking=True)
         if keep_image:
-            r.image = img.reshape(h, w, 4)
-            r.canvas = v.canvas.image.cpu().numpy().reshape(h, w, 4)   # type: ignore[attr-defined]
-            r.seeds = v.canvas.seeds.cpu().numpy().view(np.uint32).reshape(h, w)   # type: ignore[attr-defined]
-        v.release()
+            out["canvas"] = torch.empty(w * h * 4, dtype=torch.float32, pin_memory=True)
+            out["canvas"].copy_(v.canvas.image, non_blocking=True)
+            out["seeds"] = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
+            out["seeds"].copy_(v.canvas.seeds, non_blocking=True)
+        v.release()   # stream-ordered reuse: the caching allocator hands the blocks out later
+        return out
 
-    def run(self, requests: Sequence[Request], keep_images: bool = False,
-            on_step: Optional[Callable[[int], None]] = None) -> Dict[str, object]:
-        """Serve `requests` in real time (arrival times relative to the call)."""
+    def _retire(self, step, t0: float, keep_images: bool) -> int:
+        event, finishing = step
+        event.synchronize()
+        t = time.perf_counter() - t0
+        for r, out in finishing:
+            r.finished = t
+            w, h = r.view.width, r.view.height
+            if keep_images:
+                r.image = out["image"].numpy().reshape(h, w, 4)
+                r.canvas = out["canvas"].numpy().reshape(h, w, 4)   # type: ignore[attr-defined]
+                r.seeds = out["seeds"].numpy().view(np.uint32).reshape(h, w)   # type: ignore[attr-defined]
+        return len(finishing)
+
+    def _plan(self, active: Sequence[Request]):
+        """Work of the next step, at most `step_samples` samples (always at least one job):
+        interactive frames first, whole, in arrival order; then batch jobs in arrival order,
+        each up to its quantum of passes, with whatever budget is left."""
+        plan, budget = [], self.step_samples
+        for r in sorted((r for r in active if r.kind == INTERACTIVE), key=lambda r: r.arrival):
+            cost = r.view.width * r.view.height * r.view.remaining
+            if cost <= budget or not plan:
+                plan.append((r, r.view.remaining))
+                budget -= cost
+        for r in sorted((r for r in active if r.kind == BATCH), key=lambda r: r.arrival):
+            px = r.view.width * r.view.height
+            p = min(r.quantum, r.view.remaining, budget // px if px else 0)
+            if p <= 0 and not plan:
+                p = 1
+            if p > 0:
+                plan.append((r, p))
+                budget -= p * px
+        return plan
+
+    def run(self, requests: Sequence[Request], keep_images: bool = False, depth: int = 2) -> Dict[str, object]:
+        """Serve `requests` in real time (arrival times relative to the call).
+
+        Steps are planned on the host from the state the already-enqueued steps will leave
+        (which requests a step finishes is known when it is enqueued), so up to `depth` steps
+        are in flight and the host's planning, admission and read-back overlap the GPU."""
         arrivals = sorted(requests, key=lambda r: r.arrival)
         ai = 0
         waiting = collections.deque()          # arrived, not yet admitted (FIFO per class)
         waiting_i = collections.deque()
         active: List[Request] = []
+        inflight = collections.deque()
         used = 0
         t0 = time.perf_counter()
         stream = torch.cuda.current_stream(self.ctx.device)
@@ -145,33 +187,44 @@ class Server:
                     r.admitted = time.perf_counter() - t0
                     used += r.view.device_bytes()
                     active.append(r)
+            while inflight and inflight[0][0].query():
+                done += self._retire(inflight.popleft(), t0, keep_images)
             if not active:
-                if ai < len(arrivals):
-                    time.sleep(max(0.0, min(arrivals[ai].arrival - now, 0.01)))
+                if inflight:
+                    done += self._retire(inflight.popleft(), t0, keep_images)
+                elif ai < len(arrivals):
+                    time.sleep(max(0.0, min(arrivals[ai].arrival - now, 0.005)))
                 continue
-            passes = [r.view.remaining if r.kind == INTERACTIVE else min(r.quantum, r.view.remaining)
-                      for r in active]
-            self.renderer.set_views([r.view for r in active], passes, tile_pixels=self.tile_pixels,
-                                    blocks_per_sm=self.blocks_per_sm)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            if len(inflight) >= depth:
+                done += self._retire(inflight.popleft(), t0, keep_images)
+                continue
+            plan = self._plan(active)
+            self.renderer.set_views([r.view for r, _ in plan], [p for _, p in plan],
+                                    tile_pixels=self.tile_pixels, blocks_per_sm=self.blocks_per_sm)
+            e0 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             self.renderer.render()
+            e1 = torch.cuda.Event(enable_timing=True)
             e1.record(stream)
-            e1.synchronize()
-            self.device_s += e0.elapsed_time(e1) * 1e-3
+            self._step_events.append((e0, e1))
             self.steps += 1
-            if on_step:
-                on_step(self.steps)
-            still = []
-            for r, p in zip(active, passes):
+            for r, p in plan:
                 r.view.done_passes += p
+            finishing, still = [], []
+            for r in active:
                 if r.view.remaining == 0:
                     used -= r.view.device_bytes()
-                    self._finish(r, t0, keep_images)
-                    done += 1
+                    finishing.append((r, self._enqueue_finish(r, keep_images)))
                 else:
                     still.append(r)
             active = still
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            inflight.append((ev, finishing))
+        while inflight:
+            done += self._retire(inflight.popleft(), t0, keep_images)
+        torch.cuda.synchronize()
+        self.device_s = sum(a.elapsed_time(b) for a, b in self._step_events) * 1e-3
         self.renderer.check()
         return summarize(arrivals, time.perf_counter() - t0, self.device_s, self.steps)
 

@@ -146,7 +146,10 @@ typedef struct htc_batch htc_batch;
 int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out);
 void htc_batch_destroy(htc_batch *batch);
 /* Uploads the views and cuts them into tiles of `tile_pixels` pixels (most expensive views
- * first); blocks_per_sm caps residency (0 = as many as fit). Synchronises `stream`. */
+ * first); blocks_per_sm caps residency (0 = as many as fit). Asynchronous on `stream`
+ * (double-buffered pinned staging): the next launch on `stream` sees the new views, launches
+ * already enqueued keep theirs. Blocks only while the staging slot it reuses is still being
+ * copied (two calls back). */
 int htc_batch_set_views(htc_batch *batch, const htc_view *views, uint32_t n_views,
                         uint32_t tile_pixels, uint32_t blocks_per_sm, void *stream);
 /* One launch rendering every view's `passes`. stats as in htc_render_passes. */
