@@ -206,22 +206,29 @@ HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint
 // One hop (one iteration of render/scene.inl:25-41). Returns true while the path goes on.
 // `hit` reports whether the scan found an object (for the hop statistics).
 // ---------------------------------------------------------------- distance bounds
-// Any hit on object k lies on the object, so its distance is at least the distance from
-// the ray start to the object. With the world-space form of each object (staged once per
-// launch, stage_bound below) that bound costs a few FMAs, and objects whose bound exceeds
-// the best distance found so far -- widened by CULL_REL and CULL_ABS, far above the float
-// error of either side -- cannot become the nearest hit and are not tested. This changes
-// which objects are evaluated, never the result.
-//   geodesic plane:  normalised Hermitian form (A, B, C), |B|^2 - A C = 1, of the world
-//                    plane; Q(p) = A(|z|^2 + t^2) + 2 Re(B conj z) + C,
-//                    sinh(dist(p, plane)) = |Q| / (2 t)
-//   horosphere:      local height t' = t / (|n21 z + n22|^2 + |n21|^2 t^2) with N = M^-1
-//                    normalised to det 1; dist(p, horosphere) = |ln t'|
-// z = p.x + i p.y, t = p.z. Culling is off for objects with large map entries (NaN
-// records never cull) and for ray starts outside a well-conditioned box.
+// The object scan only needs the exact (reference) test for objects that can be hit nearer
+// than the best hit found so far. Whether and where the geodesic ray from (p, v) meets an
+// object has a closed form in world space, evaluated here with explicit error terms and wide
+// margins; objects it rules out are not tested. This changes which objects are evaluated,
+// never the result. Per object one float4 `rec`, staged once per launch (stage_bound):
+//   geodesic plane  rec = (A, 2Re B, 2Im B, C): the world plane's normalised Hermitian form,
+//                   |B|^2 - A C = 1. F = rec . (|p|^2, x, y, 1) = Q and sinh(signed distance
+//                   to the plane) = Q / (2t); along the unit-speed geodesic it is exactly
+//                   a cosh s + b sinh s with a = F / 2t, b = W / 2t, so the ray meets the plane
+//                   at s* = atanh(-a/b) when 0 <= -a/b < 1.
+//   horosphere      rec = (|n21|^2, 2 Re w, -2 Im w, |n22|^2), w = conj(n22) n21, N = M^-1
+//                   normalised to det 1: F = rec . (|p|^2, x, y, 1) = t / t' (t' = local
+//                   height; inside the horoball when t' > 1). Along the geodesic
+//                   1/t' = P cosh s + V sinh s with P = F / t, V = W / t; it crosses 1 at
+//                   e^s = (P - V) / (1 + r) (entry) and (1 + r) / (P + V) (exit), r^2 = 1 - P^2 + V^2.
+//   both            W = t (2 rec.x (p.v) + rec.y v.x + rec.z v.y) - F v.z
+// with p = (x, y, t) the ray start, v its unit direction (v.z along the height).
+// The threshold is thr = best (1 + CULL_REL) + CULL_ABS; objects with large map entries get
+// NaN records (never culled) and ray starts outside a well-conditioned box disable culling.
 constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
+constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
 
-struct Cull { float S, E; };   // sinh(threshold), exp(threshold); +inf = no culling
+struct Cull { float S, E, T; };   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
 
 // World-space bound record of one object from its f32 map M, in FP64 (once per launch).
 // N = adj(M) maps world to local (c22_inverse_n, matrix_complex.cc:60-65).
@@ -242,39 +249,93 @@ HT_D float4 stage_bound(const Mo &m, uint32_t shape) {
         const double Br = (n11r * n12r + n11i * n12i) - (n21r * n22r + n21i * n22i);
         const double Bi = (n11r * n12i - n11i * n12r) - (n21r * n22i - n21i * n22r);
         const double C = (n12r * n12r + n12i * n12i) - (n22r * n22r + n22i * n22i);
-        return make_float4((float)(A / adet), (float)(Br / adet), (float)(Bi / adet), (float)(C / adet));
+        return make_float4((float)(A / adet), (float)(2.0 * Br / adet), (float)(2.0 * Bi / adet), (float)(C / adet));
     }
-    const double k = 1.0 / sqrt(adet);
-    return make_float4((float)(n21r * k), (float)(n21i * k), (float)(n22r * k), (float)(n22i * k));
+    // horosphere: scale N by 1 / sqrt|det| so the height formula holds
+    const double k2 = 1.0 / adet;
+    const double c2 = (n21r * n21r + n21i * n21i) * k2;
+    const double wr = (n22r * n21r + n22i * n21i) * k2;   // w = conj(n22) n21
+    const double wi = (n22r * n21i - n22i * n21r) * k2;
+    const double n22sq = (n22r * n22r + n22i * n22i) * k2;
+    return make_float4((float)c2, (float)(2.0 * wr), (float)(-2.0 * wi), (float)n22sq);
 }
 
+// Per-hop constants of the bound evaluation.
+struct BoundRay {
+    float x, y, t, r2, pv, vx, vy, vz, ax, ay;
+};
 HT_D bool cull_point_ok(Q4 p) {
     return p.z >= 0x1p-20f && p.z <= 0x1p20f && fabsf(p.x) + fabsf(p.y) <= 0x1p10f * p.z &&
            fabsf(p.w) <= 1e-3f * p.z;
+}
+HT_D BoundRay bound_ray(Q4 p, Q4 v) {
+    BoundRay b;
+    b.x = p.x; b.y = p.y; b.t = p.z;
+    b.r2 = fmaf(p.x, p.x, fmaf(p.y, p.y, p.z * p.z));
+    b.pv = fmaf(p.x, v.x, fmaf(p.y, v.y, p.z * v.z));
+    b.vx = v.x; b.vy = v.y; b.vz = v.z;
+    b.ax = fabsf(p.x); b.ay = fabsf(p.y);
+    return b;
 }
 HT_D Cull cull_from_dist(float d) {
     const float thr = fmaf(d, 1.0f + CULL_REL, CULL_ABS);
     Cull c;
     c.S = sinhf(thr);
     c.E = expf(thr);
+    c.T = tanhf(thr);
     return c;
 }
-// true when object k provably cannot be hit nearer than the current threshold
-HT_D bool culled(float4 b, uint32_t shape, Q4 p, const Cull &c) {
-    const float x = p.x, y = p.y, t = p.z;
+HT_D Cull cull_none() {
+    Cull c;
+    c.S = c.E = __int_as_float(0x7f800000);
+    c.T = 1.0f;
+    return c;
+}
+// true when object `rec` provably cannot be hit nearer than the current threshold
+HT_D bool culled(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
+    const float t = r.t;
+    const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
+    const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+    const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
+    const float W = fmaf(t, G, -F * r.vz);
+    const float eW = fmaf(BOUND_EPS * t, fmaf(2.0f * fabsf(rec.x), fabsf(r.pv), fmaf(fabsf(rec.y), fabsf(r.vx), fabsf(rec.z * r.vy))),
+                          eF * fabsf(r.vz) + BOUND_EPS * fabsf(W));
     if (shape == 0) {
-        const float r2 = fmaf(x, x, fmaf(y, y, t * t));
-        const float q = fmaf(b.x, r2, fmaf(2.0f * b.y, x, fmaf(2.0f * b.z, y, b.w)));
-        const float err = 1e-5f * fmaf(fabsf(b.x), r2, fmaf(2.0f, fabsf(b.y * x) + fabsf(b.z * y), fabsf(b.w)));
-        return fabsf(q) - err > 2.0f * t * c.S;
+        const float Fa = fabsf(F) - eF;       // lower bound of |2 t a|
+        const float Wlo = fabsf(W) - eW, Whi = fabsf(W) + eW;
+        // starts off the plane and moves away from it: |a| > 0.01, |b| > 0.001, same signs
+        const bool away = (F > 0.0f) == (W > 0.0f) && Fa > 0.02f * t && Wlo > 0.002f * t;
+        // |a| > 1.01 T |b| + 0.01: no root (T = 1) or the root lies beyond the threshold
+        const bool far = Fa > fmaf(1.01f * c.T, Whi, 0.02f * t);
+        // the start point itself is farther than the threshold
+        const bool point = Fa > 2.0f * t * c.S;
+        return away || far || point;
     } else {
-        const float re = fmaf(b.x, x, fmaf(-b.y, y, b.z));
-        const float im = fmaf(b.x, y, fmaf(b.y, x, b.w));
-        const float cc = fmaf(b.x, b.x, b.y * b.y);
-        const float den = fmaf(re, re, fmaf(im, im, cc * t * t));
-        const float sz = (fabsf(b.x) + fabsf(b.y)) * (fabsf(x) + fabsf(y)) + fabsf(b.z) + fabsf(b.w);
-        const float err = 1e-5f * fmaf(sz, sz, cc * t * t);
-        return t > c.E * (den + err) || t * c.E < den - err;
+        // The reference accepts a root up to EPS *behind* the start before dividing by
+        // |d.xy|^2 (shape/hy/horosphere.cc:18-25), which for nearly vertical local
+        // directions means a crossing behind the ray can be reported. So the bounds hold
+        // for every point of the horosphere (point), for every crossing (no_root), for the
+        // entry when it lies ahead (entry_far), or for the nearer of both crossings when
+        // either may be reported (inside_far, away_far).
+        const float Flo = F - eF, Fhi = F + eF;
+        const float Wlo = W - eW, Whi = W + eW;
+        const float aW = fabsf(W) + eW;
+        const bool outside = Flo > 1.01f * t;    // P > 1.01
+        const bool inside = Fhi < 0.99f * t;     // P < 0.99
+        const bool approach = Whi < 0.0f;        // V < 0
+        const bool away = Wlo > 0.001f * t;      // V > 0.001
+        // K^2 = P^2 - V^2 > 1.02: the geodesic never reaches the horosphere
+        const bool no_root = Flo > 0.0f && fmaf(Flo, Flo, -aW * aW) > 1.02f * t * t;
+        // entering ahead: e^s >= (P - V) / 2 beyond the threshold
+        const bool entry_far = outside && approach && (Flo - Whi) > 2.02f * c.E * t;
+        // inside: crossings at e^s = (P - V)/(1 + r) < 1 (behind) and (1 + r)/(P + V); both
+        // farther than the threshold when (P - V) E < 1 and (P + V) E < 1
+        const bool inside_far = inside && (Fhi - Wlo) * c.E < 0.99f * t && (Fhi + Whi) * c.E < 0.99f * t;
+        // outside moving away: both crossings behind, the nearer at e^s = (1 + r)/(P + V) <= 2/(P + V)
+        const bool away_far = outside && away && (Flo + Wlo) > 2.02f * c.E * t;
+        // every point of the horosphere is farther than the threshold
+        const bool point = t > c.E * Fhi || t * c.E < Flo;
+        return no_root || entry_far || inside_far || away_far || point;
     }
 }
 
@@ -288,20 +349,20 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     uint32_t kmin = 0;
     const Q4 p = ray.p, v = ray.v;
     const bool can_cull = cull_point_ok(p);
-    Cull cull;
-    cull.S = cull.E = __int_as_float(0x7f800000);
+    const BoundRay br = bound_ray(p, v);
+    Cull cull = cull_none();
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
         const uint32_t cn = min(32u, s.n - c0);
         uint32_t mask = 0;
         for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads
             const uint32_t k = c0 + j;
-            if (!can_cull || !culled(s.bound[k], s.shape[k], p, cull)) mask |= 1u << j;
+            if (!can_cull || !culled(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
         }
         while (mask) {   // this lane's candidates, in index order
             const uint32_t k = c0 + (__ffs(mask) - 1);
             mask &= mask - 1;
             const uint32_t shape = s.shape[k];
-            if (can_cull && culled(s.bound[k], shape, p, cull)) continue;
+            if (can_cull && culled(s.bound[k], shape, br, cull)) continue;
             const bool repeat = (k == prev_hash);
             if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
             ++n_exact;
