@@ -291,6 +291,15 @@ HT_D Cull cull_none() {
     c.T = 1.0f;
     return c;
 }
+// Cheap bound: the distance from the ray start to the object alone (any hit lies on it).
+HT_D bool culled_point(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
+    const float t = r.t;
+    const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
+    const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+    if (shape == 0) return fabsf(F) - eF > 2.0f * t * c.S;
+    return t > c.E * (F + eF) || t * c.E < F - eF;
+}
+
 // true when object `rec` provably cannot be hit nearer than the current threshold
 HT_D bool culled(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
     const float t = r.t;
@@ -354,15 +363,24 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
         const uint32_t cn = min(32u, s.n - c0);
         uint32_t mask = 0;
-        for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads
+        for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads, cheap bound
             const uint32_t k = c0 + j;
-            if (!can_cull || !culled(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
+            if (!can_cull || !culled_point(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
+        }
+        if (can_cull) {   // per lane: the ray-aware bound on the survivors only
+            uint32_t m = mask;
+            while (m) {
+                const uint32_t j = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t k = c0 + j;
+                if (culled(s.bound[k], s.shape[k], br, cull)) mask &= ~(1u << j);
+            }
         }
         while (mask) {   // this lane's candidates, in index order
             const uint32_t k = c0 + (__ffs(mask) - 1);
             mask &= mask - 1;
             const uint32_t shape = s.shape[k];
-            if (can_cull && culled(s.bound[k], shape, br, cull)) continue;
+            if (can_cull && culled_point(s.bound[k], shape, br, cull)) continue;
             const bool repeat = (k == prev_hash);
             if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
             ++n_exact;
