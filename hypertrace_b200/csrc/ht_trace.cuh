@@ -226,9 +226,7 @@ HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint
 // The threshold is thr = best (1 + CULL_REL) + CULL_ABS; objects with large map entries get
 // NaN records (never culled) and ray starts outside a well-conditioned box disable culling.
 constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
-#ifndef HT_ARGMIN_FIRST
-#define HT_ARGMIN_FIRST 1
-#endif
+
 constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
 
 struct Cull { float S, E, T; };   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
@@ -363,41 +361,6 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const bool can_cull = cull_point_ok(p);
     const BoundRay br = bound_ray(p, v);
     Cull cull = cull_none();
-    uint32_t kfirst = 0xFFFFFFFFu;
-#if HT_ARGMIN_FIRST
-    // Test the object nearest to the ray start first (by a cheap sinh-distance proxy), so the
-    // threshold is tight before the scan. Only the order of the tests depends on the proxy.
-    if (can_cull) {
-        float best_lb = __int_as_float(0x7f800000);
-        for (uint32_t k = 0; k < s.n; ++k) {   // warp-uniform
-            const float4 rec = s.bound[k];
-            const float F = fmaf(rec.x, br.r2, fmaf(rec.y, br.x, fmaf(rec.z, br.y, rec.w)));
-            float lb;
-            if (s.shape[k] == 0) {
-                lb = fabsf(F) * __frcp_rn(2.0f * br.t);
-            } else {
-                const float q = F * __frcp_rn(br.t);
-                lb = 0.5f * fabsf(q - __frcp_rn(q));
-            }
-            if (lb < best_lb) { best_lb = lb; kfirst = k; }
-        }
-        if (kfirst != 0xFFFFFFFFu && !(s.shape[kfirst] == 0 && kfirst == prev_hash)) {
-            const uint32_t k = kfirst;
-            ++n_exact;
-            HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
-            const float x = s.shape[k] == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, k == prev_hash);
-            if (x >= 1.0f) {
-                const float dist = hy_dist_from_x(x);
-                if (dist > -EPSF) {
-                    min_dist = dist;
-                    min_x = x;
-                    kmin = k;
-                    cull = cull_from_dist(dist);
-                }
-            }
-        }
-    }
-#endif
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
         const uint32_t cn = min(32u, s.n - c0);
         uint32_t mask = 0;
@@ -405,7 +368,6 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
             const uint32_t k = c0 + j;
             if (!can_cull || !culled_point(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
         }
-        if (kfirst - c0 < cn) mask &= ~(1u << (kfirst - c0));   // already tested
         if (can_cull) {   // per lane: the ray-aware bound on the survivors only
             uint32_t m = mask;
             while (m) {
@@ -425,12 +387,11 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
             ++n_exact;
             HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
             const float x = shape == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, repeat);
-            // x above the best cannot give a smaller distance; it can tie it, which matters
-            // only for an index below the best's (possible when the first-tested object won)
-            if (x >= 1.0f && (x <= min_x || k < kmin)) {
+            // candidates come in index order, so x above the best's cannot win (its distance
+            // is not smaller, and a tie keeps the lower index)
+            if (x >= 1.0f && x <= min_x) {
                 const float dist = hy_dist_from_x(x);
-                // ties go to the lowest index (the first-tested object may have a higher one)
-                if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist || (dist == min_dist && k < kmin))) {
+                if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
                     min_dist = dist;
                     min_x = x;
                     kmin = k;
