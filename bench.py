@@ -221,7 +221,8 @@ def main():
     dev = ctx.device
     stream = torch.cuda.current_stream(dev)
     buf = P.EntityBuffer(ctx, sc)
-    canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed + 7919 * rank)
+    from hypertrace_b200 import replicas
+    canvas = P.Canvas(ctx, (W, H), global_seed=replicas.replica_seed(wl.global_seed, rank))
     render = P.Render(ctx, sc.recipe, sc.hops)
     stats = torch.zeros(8, dtype=torch.int64, device=dev)
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -274,13 +275,7 @@ def main():
     dev_s = sum(launch_ms) * 1e-3
     st = stats.cpu().numpy().astype(np.float64)
     samples, hops, tests, hits, exact = st[:5]
-    t = torch.tensor([dev_s], dtype=torch.float64, device=dev)
-    tot = torch.tensor([samples, hops], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    max_s = float(t.item())
-    all_samples, all_hops = [float(x) for x in tot.cpu()]
+    all_samples, max_s, all_hops = replicas.aggregate(samples, dev_s, hops, device=dev)
     value = all_samples / max_s / 1e6
 
     # roofline of the persistent kernel (one launch per step)
@@ -309,7 +304,7 @@ def main():
     # ---------------- e2e through the public API with host buffers
     e2e = None
     if not args.no_e2e:
-        pipe = P.Pipeline(ctx, (W, H), sc, global_seed=wl.global_seed + 7919 * rank)
+        pipe = P.Pipeline(ctx, (W, H), sc, global_seed=replicas.replica_seed(wl.global_seed, rank))
         host_scene = torch.frombuffer(bytearray(sc.to_bytes()), dtype=torch.uint8).pin_memory()
         host_image = torch.empty(W * H * 4, dtype=torch.uint8).pin_memory()
         for _ in range(2):
