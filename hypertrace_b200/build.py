@@ -58,6 +58,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
+EXAMPLE_SRC = os.path.join(HERE, "csrc", "examples", "render_scene.cpp")
+EXAMPLE_OUT = os.path.join(HERE, "render_scene")
+
+
+def build_example(force: bool = False) -> str:
+    """The C++ example over include/htcuda.hpp, linked against libhtcuda.so."""
+    deps = [EXAMPLE_SRC, os.path.join(ROOT, "include", "htcuda.hpp"), os.path.join(ROOT, "include", "htcuda.h"), OUT]
+    if not force and os.path.exists(EXAMPLE_OUT) and all(os.path.getmtime(d) <= os.path.getmtime(EXAMPLE_OUT) for d in deps):
+        return EXAMPLE_OUT
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", EXAMPLE_SRC, "-o", EXAMPLE_OUT,
+           "-L" + HERE, "-lhtcuda", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    return EXAMPLE_OUT
+
+
 SELFTEST_SRC = os.path.join(ROOT, "tests", "cuda", "ht_selftest.cu")
 SELFTEST_OUT = os.path.join(ROOT, "tests", "cuda", "libht_selftest.so")
 
