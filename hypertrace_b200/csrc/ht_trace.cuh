@@ -89,17 +89,7 @@ HT_D Hom hom_from(float4 a, float4 b) {
 
 // Mixture interact: one uniform draw picks the component; returns false when the path ends
 // (Emissive<Absorbing>, or the draw falls past every portion).
-#ifndef HT_COLD_NOINLINE
-#define HT_COLD_NOINLINE 1
-#endif
-#if HT_COLD_NOINLINE
-#define HT_COLD __device__ __noinline__
-#else
-#define HT_COLD HT_D
-#endif
-
-// Once per hop, not in the scan: kept out of line (instruction-cache footprint).
-HT_COLD bool mixture_interact(const Material &m, uint32_t &rng, V3 normal, V3 &dir, Col &intensity,
+HT_D bool mixture_interact(const Material &m, uint32_t &rng, V3 normal, V3 &dir, Col &intensity,
                            Col &emission) {
     float alpha = rng_uniform(rng);
     alpha -= m.diffuse;
@@ -200,7 +190,7 @@ HT_D void horosphere_hit(Q4 p, Q4 d, bool repeat, HyPath &hit, Q4 &normal) {
 
 // Camera ray: view/point/impl.inl:18-25 (hy_origin = j, hyperbolic.cc:4-6) then the
 // camera Moebius map (view/mapped.inl:20-26).
-HT_COLD HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
+HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
     float u0 = rng_uniform(rng);
     float u1 = rng_uniform(rng);
     float jx = (flags & FLAG_JITTER_YX) ? u1 : u0;
@@ -239,20 +229,7 @@ constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
 
 constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
 
-struct Cull { float S, E, T; };
-
-#ifndef HT_CHUNK64
-#define HT_CHUNK64 0
-#endif
-#if HT_CHUNK64
-typedef unsigned long long ChunkMask;
-constexpr uint32_t CHUNK = 64;
-HT_D int mask_ffs(ChunkMask m) { return __ffsll((long long)m); }
-#else
-typedef uint32_t ChunkMask;
-constexpr uint32_t CHUNK = 32;
-HT_D int mask_ffs(ChunkMask m) { return __ffs(m); }
-#endif   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
+struct Cull { float S, E, T; };   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
 
 // World-space bound record of one object from its f32 map M, in FP64 (once per launch).
 // N = adj(M) maps world to local (c22_inverse_n, matrix_complex.cc:60-65).
@@ -384,24 +361,24 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const bool can_cull = cull_point_ok(p);
     const BoundRay br = bound_ray(p, v);
     Cull cull = cull_none();
-    for (uint32_t c0 = 0; c0 < s.n; c0 += CHUNK) {
-        const uint32_t cn = min(CHUNK, s.n - c0);
-        ChunkMask mask = 0;
+    for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
+        const uint32_t cn = min(32u, s.n - c0);
+        uint32_t mask = 0;
         for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads, cheap bound
             const uint32_t k = c0 + j;
-            if (!can_cull || !culled_point(s.bound[k], s.shape[k], br, cull)) mask |= (ChunkMask)1 << j;
+            if (!can_cull || !culled_point(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
         }
         if (can_cull) {   // per lane: the ray-aware bound on the survivors only
-            ChunkMask m = mask;
+            uint32_t m = mask;
             while (m) {
-                const uint32_t j = mask_ffs(m) - 1;
+                const uint32_t j = __ffs(m) - 1;
                 m &= m - 1;
                 const uint32_t k = c0 + j;
-                if (culled(s.bound[k], s.shape[k], br, cull)) mask &= ~((ChunkMask)1 << j);
+                if (culled(s.bound[k], s.shape[k], br, cull)) mask &= ~(1u << j);
             }
         }
         while (mask) {   // this lane's candidates, in index order
-            const uint32_t k = c0 + (mask_ffs(mask) - 1);
+            const uint32_t k = c0 + (__ffs(mask) - 1);
             mask &= mask - 1;
             const uint32_t shape = s.shape[k];
             if (can_cull && culled_point(s.bound[k], shape, br, cull)) continue;
@@ -475,7 +452,7 @@ HT_D float plane_eu_dist(V3 pos, V3 dir) {   // shape/eu/plane.cc:3-21 (repeat h
     return -pos.z / dir.z;
 }
 
-HT_COLD EuPath camera_eu(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
+HT_D EuPath camera_eu(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
     float u0 = rng_uniform(rng);
     float u1 = rng_uniform(rng);
     float jx = (flags & FLAG_JITTER_YX) ? u1 : u0;
