@@ -14,8 +14,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "htcuda.cu")
+SRCS = [os.path.join(HERE, "csrc", "htcuda.cu"), os.path.join(HERE, "csrc", "htgeneric.cu")]
 OUT = os.path.join(HERE, "libhtcuda.so")
+# Device headers that htc_program_build hands to NVRTC, embedded as C strings.
+NVRTC_HEADERS = [("k_header_ht_math", "ht_math.cuh"), ("k_header_ht_generic", "ht_generic.cuh")]
+GENERATED = os.path.join(HERE, "csrc", "generated", "nvrtc_headers.inc")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -36,7 +39,7 @@ def nvcc() -> str:
 def sources():
     csrc = os.path.join(HERE, "csrc")
     return [os.path.join(csrc, f) for f in sorted(os.listdir(csrc))
-            if f.endswith((".cu", ".cuh", ".h"))] + [os.path.join(ROOT, "include", "htcuda.h")]
+            if f.endswith((".cu", ".cuh", ".h", ".hpp"))] + [os.path.join(ROOT, "include", "htcuda.h"), GENERATED]
 
 
 def up_to_date() -> bool:
@@ -46,10 +49,34 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
+def c_string(text: str) -> str:
+    out = []
+    for line in text.splitlines(True):
+        esc = line.replace("\\", "\\\\").replace('"', '\\"').replace("\n", "\\n")
+        out.append('"' + esc + '"')
+    return "\n".join(out) if out else '""'
+
+
+def gen_headers() -> str:
+    """Writes csrc/generated/nvrtc_headers.inc (the NVRTC header texts) when stale."""
+    os.makedirs(os.path.dirname(GENERATED), exist_ok=True)
+    parts = ["// generated by hypertrace_b200/build.py from the files named below; do not edit\n"]
+    for var, name in NVRTC_HEADERS:
+        with open(os.path.join(HERE, "csrc", name)) as f:
+            parts.append("// %s\nstatic const char %s[] =\n%s;\n" % (name, var, c_string(f.read())))
+    text = "".join(parts)
+    old = open(GENERATED).read() if os.path.exists(GENERATED) else None
+    if old != text:
+        with open(GENERATED, "w") as f:
+            f.write(text)
+    return GENERATED
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    gen_headers()
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", OUT, SRC]
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", OUT] + SRCS
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)

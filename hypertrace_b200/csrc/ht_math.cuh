@@ -6,7 +6,16 @@
 // bit-identical to the reference compiled for the host. Transcendentals are the
 // exception: they come from CUDA's libdevice (cos/sin evaluated in FP64, see below).
 #pragma once
+#ifdef __CUDACC_RTC__
+// Runtime compilation (NVRTC) has no C++ standard headers; these are the only ones used.
+typedef unsigned char uint8_t;
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+typedef int int32_t;
+typedef unsigned long long uintptr_t;
+#else
 #include <cstdint>
+#endif
 
 namespace ht {
 
@@ -104,7 +113,7 @@ HT_D Q4 normalize4_fast(Q4 a, bool &bad) {
 struct HyRay { Q4 p, v; };
 
 // Reference evaluation with IEEE division everywhere (the fallback of ray_hy_map).
-__device__ __noinline__ HyRay ray_hy_map_ieee(const Mo m, const Q4 p, const Q4 v) {
+static __device__ __noinline__ HyRay ray_hy_map_ieee(const Mo m, const Q4 p, const Q4 v) {
     Q4 u = q_addc(cq_mul(m.a, p), m.b);
     Q4 d = q_addc(cq_mul(m.c, p), m.d);
     float d2 = dot4(d, d);
@@ -149,7 +158,7 @@ HT_D HyRay ray_hy_map(const Mo &m, Q4 p, Q4 v) {
 }
 // The same map, out of line: used by the once-per-hop winner path so that only the scan
 // keeps an inlined copy (instruction-cache footprint).
-__device__ __noinline__ HyRay ray_hy_map_call(const Mo m, const Q4 p, const Q4 v) { return ray_hy_map(m, p, v); }
+static __device__ __noinline__ HyRay ray_hy_map_call(const Mo m, const Q4 p, const Q4 v) { return ray_hy_map(m, p, v); }
 
 // Camera map (view/mapped.inl:20-26): direction = mo_apply_dir (one normalize), then start.
 // Once per sample, so plain IEEE division.

@@ -24,25 +24,12 @@
 
 #include "../../include/htcuda.h"
 #include "ht_trace.cuh"
+#include "ht_host.hpp"
 
 using namespace ht;
 
 // ============================================================================ errors
-static thread_local std::string g_last_error;
-
-static int fail(int code, const std::string &msg) {
-    g_last_error = msg;
-    return code;
-}
-static int cuda_fail(cudaError_t e, const char *what) {
-    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
-    return HTC_ERR_CUDA;
-}
-#define HTC_CUDA(call)                                  \
-    do {                                                \
-        cudaError_t e_ = (call);                        \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-    } while (0)
+thread_local std::string g_last_error;
 
 // Minimum resident blocks per SM requested from ptxas for the render kernels (register cap).
 // Six 128-thread blocks per SM (80 registers) measured fastest for both kernels: the scan
@@ -68,6 +55,7 @@ struct htc_program {
     uint32_t *d_queue;   // [0] next pixel, [1] finished blocks (persistent kernel)
     int num_sms;
     int max_smem;
+    GenericProgram *generic;   // scene types served by render_generic (htgeneric.cu), else NULL
 };
 
 // ============================================================================ staging
@@ -532,6 +520,27 @@ static int validate_render_args(htc_program *p, uint32_t W, uint32_t H, const vo
     return HTC_OK;
 }
 
+// A program around a generic scene kernel: error word only (no staging, no queue).
+static int wrap_generic(GenericProgram *g, int recipe, uint32_t light_hops, int address_width, uint32_t flags,
+                        htc_program **out) {
+    htc_program *p = new htc_program();
+    p->recipe = recipe;
+    p->hops = light_hops;
+    p->address_width = address_width;
+    p->flags = flags;
+    p->generic = g;
+    cudaError_t e = cudaMalloc(&p->d_err, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        if (p->d_err) cudaFree(p->d_err);
+        generic_program_destroy(g);
+        delete p;
+        return cuda_fail(e, "htc_program_create");
+    }
+    *out = p;
+    return HTC_OK;
+}
+
 extern "C" {
 
 const char *htc_last_error(void) { return g_last_error.c_str(); }
@@ -551,11 +560,19 @@ int htc_program_create(int recipe, uint32_t light_hops, int address_width, int d
                        uint32_t flags, htc_program **out) {
     if (!out) return fail(HTC_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    if (recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU) return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
+    if (recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU && recipe != HTC_RECIPE_HY_TILED &&
+        recipe != HTC_RECIPE_EU_GRADIENT)
+        return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
     if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
     if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
     if (double_support) return fail(HTC_ERR_UNSUPPORTED, "double_support scenes are not served (f32 transport)");
     if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    if (recipe == HTC_RECIPE_HY_TILED || recipe == HTC_RECIPE_EU_GRADIENT) {
+        GenericProgram *g = nullptr;
+        int rc = generic_program_create(recipe, address_width, &g);
+        if (rc) return rc;
+        return wrap_generic(g, recipe, light_hops, address_width, flags, out);
+    }
     int dev = 0;
     HTC_CUDA(cudaGetDevice(&dev));
     htc_program *p = new htc_program();
@@ -590,8 +607,32 @@ int htc_program_create(int recipe, uint32_t light_hops, int address_width, int d
 void htc_program_destroy(htc_program *p) {
     if (!p) return;
     cudaFree(p->d_err);
-    cudaFree(p->d_queue);
+    if (p->d_queue) cudaFree(p->d_queue);
+    if (p->generic) generic_program_destroy(p->generic);
     delete p;
+}
+
+int htc_program_build(const char *scene_type, uint32_t light_hops, int address_width, uint32_t flags, char *log,
+                      size_t log_len, htc_program **out) {
+    if (!out) return fail(HTC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene_type || !scene_type[0]) return fail(HTC_ERR_INVALID, "scene_type is empty");
+    if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
+    if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
+    if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    GenericProgram *g = nullptr;
+    int rc = generic_program_build(scene_type, address_width, log, log_len, &g);
+    if (rc) return rc;
+    return wrap_generic(g, HTC_RECIPE_CUSTOM, light_hops, address_width, flags, out);
+}
+
+int htc_program_static_size(const htc_program *p, uint64_t *bytes) {
+    int rc = check_program(p);
+    if (rc) return rc;
+    if (!bytes) return fail(HTC_ERR_INVALID, "bytes is NULL");
+    if (p->generic) *bytes = generic_min_size(p->generic);
+    else *bytes = p->recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
+    return HTC_OK;
 }
 
 int htc_program_check(htc_program *p, void *stream) {
@@ -636,8 +677,22 @@ int htc_stream_sync(void *stream) {
     return HTC_OK;
 }
 
+// Argument checks and launch of a generic scene program (passes samples per pixel).
+static int render_generic_program(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                                  float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+    if (W == 0 || H == 0) return fail(HTC_ERR_INVALID, "canvas width and height must be positive");
+    if ((uint64_t)W * (uint64_t)H >= 0xFFFFFFFFull) return fail(HTC_ERR_INVALID, "canvas too large (W*H must fit in 32 bits)");
+    if (!scene || !canvas || !seeds) return fail(HTC_ERR_INVALID, "scene, canvas and seeds must be device pointers");
+    if ((reinterpret_cast<uintptr_t>(scene) & 31u) != 0 || (reinterpret_cast<uintptr_t>(canvas) & 15u) != 0)
+        return fail(HTC_ERR_INVALID, "scene must be 32-byte and canvas 16-byte aligned");
+    if (passes == 0) return HTC_OK;
+    return generic_render(p->generic, W, H, p->hops, p->flags, scene, scene_size, canvas, seeds, passes, stats,
+                          p->d_err, stream);
+}
+
 int htc_render_ex(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
                   float *canvas, uint32_t *seeds, uint64_t *stats, void *stream) {
+    if (p && p->generic) return render_generic_program(p, W, H, scene, scene_size, canvas, seeds, 1, stats, stream);
     uint32_t max_objects = 0;
     size_t smem = 0;
     int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
@@ -663,6 +718,7 @@ int htc_render(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t
 
 int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
                       float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+    if (p && p->generic) return render_generic_program(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
     uint32_t max_objects = 0;
     size_t smem = 0;
     int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);

@@ -40,6 +40,21 @@ extern "C" {
  */
 #define HTC_RECIPE_HY 1
 #define HTC_RECIPE_EU 2
+/* Scene types served by the generic template kernels (compiled into the library):
+ *   HTC_RECIPE_HY_TILED     SceneImpl<Hyperbolic3, Mapped<PointView, Moebius>,
+ *                             Vec<Mapped<Choice{TiledPlane<M, Pentastar, 2>,
+ *                               TiledPlane<M, Pentagonal, 2>, TiledHorosphere<M, Hexagonal, 3>,
+ *                               TiledHorosphere<M, Square, 4>}, Moebius>>, ConstBg, H>,
+ *                           M = Emissive<Mixture{Colored<Lambertian>, Specular, Transparent}>
+ *                                                        (main/examples/hy.rs:35-75)
+ *   HTC_RECIPE_EU_GRADIENT  SceneImpl<Euclidean3, Mapped<PointView, Homogenous3>,
+ *                             Vec<Mapped<Covered<Choice{Plane, Sphere, Cube},
+ *                               Mixture{Colored<Lambertian>, Specular, Colored<Refractive>}>,
+ *                               Shift3>>, GradBg, H>   (main/examples/eu.rs:30-44)
+ * HTC_RECIPE_CUSTOM is the recipe of a program made by htc_program_build. */
+#define HTC_RECIPE_HY_TILED 3
+#define HTC_RECIPE_EU_GRADIENT 4
+#define HTC_RECIPE_CUSTOM 100
 
 /* Program flags. */
 #define HTC_FLAG_JITTER_YX 1u  /* first pixel-jitter draw goes to y: the order in which g++
@@ -70,6 +85,18 @@ int htc_set_device(int device);
 int htc_program_create(int recipe, uint32_t light_hops, int address_width, int double_support,
                        uint32_t flags, htc_program **out);
 void htc_program_destroy(htc_program *program);
+/* Replaces the source generation and ocl::Program::build of Render::new
+ * (processing/src/render.rs:14-100, types/src/source.rs:102-168) for any scene type:
+ * `scene_type` is the C++ type expression of the scene over the templates of
+ * hypertrace_b200/csrc/ht_generic.cuh (e.g. "SceneImpl<Eu, MappedView<Eu, PointView<Eu>,
+ * Homogenous3>, ObjectVec<Eu, ...>, ConstBg>", as hypertrace_b200/types.py writes it),
+ * compiled at run time with NVRTC for sm_100a. The compiler log goes to `log` (may be
+ * NULL). The program renders with htc_render / htc_render_ex / htc_render_passes. */
+int htc_program_build(const char *scene_type, uint32_t light_hops, int address_width, uint32_t flags,
+                      char *log, size_t log_len, htc_program **out);
+/* Serialized size of the program's scene type without its dynamic part (for a Vec of
+ * objects: the bytes up to the first element); a smaller scene buffer is rejected. */
+int htc_program_static_size(const htc_program *program, uint64_t *bytes);
 /* Reads and clears the device-side error word of the program's last launches
  * (synchronises `stream`). Returns HTC_OK or HTC_ERR_SCENE / HTC_ERR_TIMEOUT. */
 int htc_program_check(htc_program *program, void *stream);
