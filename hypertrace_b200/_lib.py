@@ -22,6 +22,9 @@ HTC_ERR_TIMEOUT = -6
 
 HTC_RECIPE_HY = 1
 HTC_RECIPE_EU = 2
+HTC_RECIPE_HY_TILED = 3
+HTC_RECIPE_EU_GRADIENT = 4
+HTC_RECIPE_CUSTOM = 100
 HTC_FLAG_JITTER_YX = 1
 
 STAT_SAMPLES, STAT_HOPS, STAT_OBJECT_TESTS, STAT_HITS = 0, 1, 2, 3
@@ -39,6 +42,8 @@ SIGNATURES = [
     ("htc_set_device", _i, [_i]),
     ("htc_program_create", _i, [_i, _u32, _i, _i, _u32, ctypes.POINTER(_vp)]),
     ("htc_program_destroy", None, [_vp]),
+    ("htc_program_build", _i, [ctypes.c_char_p, _u32, _i, _u32, ctypes.c_char_p, _sz, ctypes.POINTER(_vp)]),
+    ("htc_program_static_size", _i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     ("htc_program_check", _i, [_vp, _vp]),
     ("htc_malloc", _i, [ctypes.POINTER(_vp), _sz]),
     ("htc_free", _i, [_vp]),
