@@ -573,7 +573,8 @@ struct GradBg {   // {direction, colors[2], power} (background/basic.rs:54-58), 
         const Col c0 = ldc3(self + 16), c1 = ldc3(self + 32);
         const float power = ldf(self + 48);
         float f = 0.5f * (dot3(l.v, dir) + 1.0f);
-        f = fminf(fmaxf(f, 0.0f), 1.0f);
+        f = (f < 0.0f) ? 0.0f : f;   // clamp = min(max(f, 0), 1) with std::max / std::min (math.hh)
+        f = (1.0f < f) ? 1.0f : f;
         f = powf_rounded(f, power);
         const float g = 1.0f - f;
         e.x += (f * c0.x + g * c1.x) * l.k.x;

@@ -579,3 +579,124 @@ def hearth_value(scene) -> dict:
             for o in scene.objects]
     return {"view": {"map": _map_value(scene.camera), "inner": {"fov": scene.fov}},
             "background": {"color": scene.background}, "object": objs}
+
+
+# ----------------------------------------------------------------------------- example scenes
+
+def _unpack_color(rgb: int) -> np.ndarray:
+    """unpack_color + make_color of main/examples/hy.rs:27-33 (sRGB byte -> linear, power 2.2)."""
+    v = np.array([(rgb >> 16) & 0xFF, (rgb >> 8) & 0xFF, rgb & 0xFF], dtype=np.float32) / np.float32(255.0)
+    return np.power(v, np.float32(2.2)).astype(np.float32)
+
+
+def _hy_material(diffuse, specularity: float, transparency: float, emission=None) -> dict:
+    """make_material of main/examples/hy.rs:43-62."""
+    return {"emission": (0.0, 0.0, 0.0) if emission is None else emission,
+            "inner": {"diffuse": {"material": {"color": diffuse, "inner": None},
+                                  "portion": 1.0 - specularity - transparency},
+                      "specular": {"material": None, "portion": specularity},
+                      "transparent": {"material": None, "portion": transparency}}}
+
+
+def hy_example_camera() -> np.ndarray:
+    """The controller's initial map in main/examples/hy.rs:143-148:
+    rotate_z(5 pi / 6) . rotate_x(2 pi / 5) . shift_z(2)."""
+    from . import scene as S
+    return S.mo_chain(S.mo_chain(S.mo_zrotate(5 * np.pi / 6), S.mo_xrotate(2 * np.pi / 5)), S.mo_zshift(2.0))
+
+
+def hy_example_value(camera=None, fov: float = 1.0) -> dict:
+    """The scene of main/examples/hy.rs:103-139 (value of hy_tiled_type())."""
+    from . import scene as S
+    border = _hy_material(_unpack_color(0xE4E4E4), 0.0, 0.0, np.ones(3, dtype=np.float32))
+    m = lambda rgb, s, t: _hy_material(_unpack_color(rgb), s, t)
+    ident = S.mo_identity()
+    shift2 = np.array([[1.0, np.sqrt(2.0)], [0.0, 1.0]], dtype=np.complex128)
+    objs = [
+        {"map": ident, "inner": ("HoroHexa", {"materials": [m(0xFE0000, .1, .1), m(0xFFAA01, .1, .1), m(0x35ADAE, .1, .1)],
+                                              "border_material": border, "cell_size": 0.5, "border_width": 0.02})},
+        {"map": S.mo_chain(shift2, S.mo_xrotate(np.pi)),
+         "inner": ("HoroSquare", {"materials": [m(0xFE7401, .1, .1), m(0xFE0000, .1, .1), m(0xFFAA01, .1, .1),
+                                                m(0xFED601, .1, .1)],
+                                  "border_material": border, "cell_size": 0.5, "border_width": 0.02})},
+        {"map": ident, "inner": ("PlaneStar", {"materials": [m(0xFE7401, .1, 0.0), m(0x35ADAE, .1, 0.0)],
+                                               "border_material": border, "cell_size": float("nan"),
+                                               "border_width": 0.01})},
+        {"map": np.array([[1.0, 2.0j], [0.0, 1.0]], dtype=np.complex128),
+         "inner": ("PlanePenta", {"materials": [m(0xFE0000, .1, 0.0), m(0xFED601, .1, 0.0)],
+                                  "border_material": border, "cell_size": float("nan"), "border_width": 0.02})},
+    ]
+    cam = hy_example_camera() if camera is None else camera
+    return {"view": {"map": cam, "inner": {"fov": fov}}, "background": {"color": _unpack_color(0xEEEEEE)},
+            "object": objs}
+
+
+def eu_example_value(camera=None, fov: float = 1.0) -> dict:
+    """The scene of main/examples/eu.rs:71-122 (value of eu_gradient_type()); the camera is
+    the controller's initial map, a shift by (0, 0.5, 2) (eu.rs:134-140)."""
+    def mix(dc, dp, sp, rc, ri, rp):
+        return {"diffuse": {"material": {"color": dc, "inner": None}, "portion": dp},
+                "specular": {"material": None, "portion": sp},
+                "refractive": {"material": {"color": rc, "inner": {"index": ri}}, "portion": rp}}
+    objs = [
+        {"map": (0.0, 1.0, 0.0), "inner": {"material": mix((1.0, 0.2, 0.2), 0.0, 0.1, (1.0, 1.0, 0.2), 1.2, 0.9),
+                                           "shape": ("Sphere", None)}},
+        {"map": (0.0, -1.0, 0.0), "inner": {"material": mix((0.2, 0.8, 0.8), 1.0, 0.0, (1.0, 1.0, 1.0), 1.0, 0.0),
+                                            "shape": ("Cube", None)}},
+        {"map": (0.0, 0.0, -1.0), "inner": {"material": mix((1.0, 1.0, 1.0), 0.9, 0.1, (1.0, 1.0, 1.0), 1.0, 0.0),
+                                            "shape": ("Plane", None)}},
+    ]
+    cam = ((0.0, 0.5, 2.0), (1.0, 0.0, 0.0, 0.0)) if camera is None else camera
+    return {"view": {"map": cam, "inner": {"fov": fov}},
+            "background": {"direction": (0.0, 1.0, 0.0), "colors": [(1.0, 1.0, 1.0), (0.0, 0.0, 0.0)], "power": 2.4},
+            "object": objs}
+
+
+def hy_tiled_random_value(seed: int, n_objects: int = 8, max_distance: float = 2.0) -> dict:
+    """A random scene of hy_tiled_type(): n tiled objects of random variants, random maps
+    (translation <= max_distance), random materials and camera."""
+    from . import scene as S
+    rng = np.random.default_rng(seed)
+
+    def mat(emissive: bool = False):
+        s, t = float(rng.uniform(0, 0.4)), float(rng.uniform(0, 0.4))
+        em = tuple(rng.uniform(0.5, 3.0, 3)) if emissive else None
+        return _hy_material(tuple(rng.uniform(0.1, 0.9, 3)), s, t, em)
+    counts = {"PlaneStar": 2, "PlanePenta": 2, "HoroHexa": 3, "HoroSquare": 4}
+    names = list(counts)
+    objs = []
+    for _ in range(n_objects):
+        v = names[int(rng.integers(4))]
+        body = {"materials": [mat() for _ in range(counts[v])], "border_material": mat(emissive=bool(rng.integers(2))),
+                "cell_size": float(rng.uniform(0.2, 1.0)) if v.startswith("Horo") else float("nan"),
+                "border_width": float(rng.uniform(0.005, 0.05))}
+        objs.append({"map": S.random_moebius(rng, max_distance), "inner": (v, body)})
+    return {"view": {"map": S.random_moebius(rng, 1.0), "inner": {"fov": float(rng.uniform(0.6, 1.5))}},
+            "background": {"color": tuple(rng.uniform(0.2, 1.0, 3))}, "object": objs}
+
+
+def eu_gradient_random_value(seed: int, n_objects: int = 8) -> dict:
+    """A random scene of eu_gradient_type(): planes, spheres and cubes shifted around the
+    origin, random mixtures (refractive indices in [1, 2]), a random camera in front."""
+    from . import scene as S
+    rng = np.random.default_rng(seed)
+    objs = []
+    for i in range(n_objects):
+        shape = ("Plane", "Sphere", "Cube")[0 if i == 0 else int(rng.integers(1, 3))]
+        p = rng.dirichlet([1.0, 1.0, 1.0])
+        objs.append({"map": (0.0, 0.0, -1.5) if i == 0 else tuple(rng.uniform(-3, 3, 2)) + (float(rng.uniform(-1, 2)),),
+                     "inner": {"material": {
+                         "diffuse": {"material": {"color": tuple(rng.uniform(0.1, 0.9, 3)), "inner": None}, "portion": float(p[0])},
+                         "specular": {"material": None, "portion": float(p[1])},
+                         "refractive": {"material": {"color": tuple(rng.uniform(0.5, 1.0, 3)),
+                                                     "inner": {"index": float(rng.uniform(1.0, 2.0))}},
+                                        "portion": float(p[2])}},
+                         "shape": (shape, None)}})
+    q = S.quat_axis_angle([1.0, 0.0, 0.0], float(rng.uniform(-0.3, 0.3)))
+    cam = ((float(rng.uniform(-1, 1)), float(rng.uniform(-1, 1)), float(rng.uniform(5, 8))), tuple(q))
+    d = rng.normal(size=3)
+    return {"view": {"map": cam, "inner": {"fov": float(rng.uniform(0.6, 1.5))}},
+            "background": {"direction": tuple(d / np.linalg.norm(d)),
+                           "colors": [tuple(rng.uniform(0.5, 1.5, 3)), tuple(rng.uniform(0.0, 0.3, 3))],
+                           "power": float(rng.uniform(0.5, 4.0))},
+            "object": objs}

@@ -577,9 +577,16 @@ static void *worker_main(void *arg) {
 /* Renders `passes` passes over the listed pixels; same contract as htref_render.
  * Returns 0, or a negative error (-1 short/bad scene, -2 unknown recipe, -3 bad hops,
  * -4 bad address width, -5 bad shape index). */
+static int render_ext(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, int address_width,
+                      uint32_t W, uint32_t H, const uint32_t *pixels, size_t n_pixels, uint32_t passes,
+                      float *canvas, uint32_t *seeds, uint32_t flags, int threads, uint64_t *stats);
+
 int HTO(render)(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, int address_width,
                 uint32_t W, uint32_t H, const uint32_t *pixels, size_t n_pixels, uint32_t passes,
                 float *canvas, uint32_t *seeds, uint32_t flags, int threads, uint64_t *stats) {
+    if (recipe == 3 || recipe == 4)
+        return render_ext(recipe, hops, scene, scene_len, address_width, W, H, pixels, n_pixels, passes, canvas,
+                          seeds, flags, threads, stats);
     if (hops == 0) return -3;
     if (W == 0 || H == 0) return -1;
     scene_t sc;
@@ -630,4 +637,578 @@ void HTO(rng_uniforms)(uint32_t seed, uint32_t n, double *out, uint32_t *state_o
     uint32_t s = seed;
     for (uint32_t i = 0; i < n; ++i) out[i] = (double)rng_uniform(&s);
     if (state_out) *state_out = s;
+}
+
+/* ======================================================================================
+ * The scene types of the reference's hy and eu examples (recipes 3 and 4).
+ *
+ *   3: SceneImpl<Hyperbolic3, Mapped<PointView, Moebius>, Vec<Mapped<Choice{
+ *        TiledPlane<M, Pentastar, 2>, TiledPlane<M, Pentagonal, 2>,
+ *        TiledHorosphere<M, Hexagonal, 3>, TiledHorosphere<M, Square, 4>}, Moebius>>, ConstBg, H>
+ *      M = Emissive<Mixture{Colored<Lambertian>, Specular, Transparent}>  (main/examples/hy.rs)
+ *   4: SceneImpl<Euclidean3, Mapped<PointView, Homogenous3>, Vec<Mapped<Covered<
+ *        Choice{Plane, Sphere, Cube}, Mixture{Colored<Lambertian>, Specular,
+ *        Colored<Refractive>}>, Shift3>>, GradBg, H>                      (main/examples/eu.rs)
+ *
+ * Byte offsets (from the layout rules of type-macros/src/entity.rs, as written by
+ * hypertrace_b200/types.py; identical for address width 32 and 64):
+ *   3: view map @0, fov @32, background @64, count @96, objects @128 + 384 i;
+ *      object: map @0, variant index @32, payload @48 = N materials of 64 bytes, border
+ *      material, cell_size, border_width; material: emission @0, diffuse color @16,
+ *      diffuse portion @32, specular portion @48, transparent portion @52.
+ *   4: view Homogenous3 @0, fov @32, GradBg{direction @48, colors @64 @80, power @96},
+ *      count @112, objects @128 + 128 i; object: shift @0, diffuse color @16, diffuse
+ *      portion @32, specular portion @48, refractive color @64, index @80, portion @96,
+ *      shape index @112.
+ * ====================================================================================== */
+
+typedef struct {
+    col3 emission;
+    col3 diffuse_color; R diffuse, specular, transparent;
+} tl_material;
+
+typedef struct {
+    moebius map, inv;
+    uint32_t variant;
+    tl_material mats[4];
+    tl_material border;
+    R cell_size, border_width;
+} tl_object;
+
+typedef struct {
+    col3 diffuse_color; R diffuse, specular;
+    col3 refr_color; R refr_index, refr;
+    vec3 shift, shift_inv;
+    uint32_t shape;
+} gr_object;
+
+typedef struct {
+    int recipe;
+    uint32_t n;
+    R fov;
+    moebius cam_mo;
+    hom3 cam_hom;
+    col3 background;
+    vec3 grad_dir; col3 grad_c0, grad_c1; float grad_power;
+    tl_object *tl;
+    gr_object *gr;
+} ext_scene_t;
+
+static col3 rd_col(const uint8_t *b, size_t off) { col3 c = {rd_f(b, off), rd_f(b, off + 4), rd_f(b, off + 8)}; return c; }
+
+static tl_material rd_tl_material(const uint8_t *b) {
+    tl_material m;
+    m.emission = rd_col(b, 0);
+    m.diffuse_color = rd_col(b, 16);
+    m.diffuse = rd_f(b, 32);
+    m.specular = rd_f(b, 48);
+    m.transparent = rd_f(b, 52);
+    return m;
+}
+
+static int ext_parse(int recipe, const uint8_t *b, size_t len, int aw, ext_scene_t *s) {
+    memset(s, 0, sizeof(*s));
+    if (aw != 32 && aw != 64) return -4;
+    s->recipe = recipe;
+    if (len < 128) return -1;
+    s->fov = rd_f(b, 32);
+    if (recipe == 3) {
+        static const uint32_t counts[4] = {2, 2, 3, 4};
+        s->cam_mo = rd_mo(b);
+        s->background = rd_col(b, 64);
+        s->n = rd_u(b, 96);
+        if (aw == 64 && rd_u(b, 100) != 0) return -1;
+        if ((len - 128) / 384 < s->n) return -1;
+        s->tl = (tl_object *)calloc(s->n ? s->n : 1, sizeof(tl_object));
+        for (uint32_t i = 0; i < s->n; ++i) {
+            const uint8_t *o = b + 128 + (size_t)i * 384;
+            tl_object *t = &s->tl[i];
+            t->map = rd_mo(o);
+            t->inv = mo_inverse(t->map);
+            t->variant = rd_u(o, 32);
+            if ((aw == 64 && rd_u(o, 36) != 0) || t->variant > 3) { free(s->tl); return -5; }
+            const uint32_t nm = counts[t->variant];
+            for (uint32_t k = 0; k < nm; ++k) t->mats[k] = rd_tl_material(o + 48 + 64 * k);
+            t->border = rd_tl_material(o + 48 + 64 * nm);
+            t->cell_size = rd_f(o, 48 + 64 * nm + 64);
+            t->border_width = rd_f(o, 48 + 64 * nm + 68);
+        }
+        return 0;
+    }
+    s->cam_hom = rd_hom(b);
+    s->grad_dir = v3(rd_f(b, 48), rd_f(b, 52), rd_f(b, 56));
+    s->grad_c0 = rd_col(b, 64);
+    s->grad_c1 = rd_col(b, 80);
+    s->grad_power = rd_f(b, 96);
+    s->n = rd_u(b, 112);
+    if (aw == 64 && rd_u(b, 116) != 0) return -1;
+    if ((len - 128) / 128 < s->n) return -1;
+    s->gr = (gr_object *)calloc(s->n ? s->n : 1, sizeof(gr_object));
+    for (uint32_t i = 0; i < s->n; ++i) {
+        const uint8_t *o = b + 128 + (size_t)i * 128;
+        gr_object *g = &s->gr[i];
+        g->shift = v3(rd_f(o, 0), rd_f(o, 4), rd_f(o, 8));
+        g->shift_inv = v3(-g->shift.x, -g->shift.y, -g->shift.z);   /* shf3_inverse (shift.cc) */
+        g->diffuse_color = rd_col(o, 16);
+        g->diffuse = rd_f(o, 32);
+        g->specular = rd_f(o, 48);
+        g->refr_color = rd_col(o, 64);
+        g->refr_index = rd_f(o, 80);
+        g->refr = rd_f(o, 96);
+        g->shape = rd_u(o, 112);
+        if ((aw == 64 && rd_u(o, 116) != 0) || g->shape > 2) { free(s->gr); return -5; }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ materials (shared) */
+static inline void lambertian(uint32_t *rng, vec3 normal, vec3 *dir) {   /* lambertian.cc:6-14 */
+    if (dot3(*dir, normal) > (R)0) normal = v3(-normal.x, -normal.y, -normal.z);
+    vec3 rnd = hemisphere_cosine(rng);
+    quat rot = rot3_look_at(v3(-normal.x, -normal.y, -normal.z));
+    *dir = rot3_apply(rot, rnd);
+}
+static inline void specular(vec3 normal, vec3 *dir) {   /* specular.cc:4-7 */
+    R k = (R)2 * dot3(*dir, normal);
+    *dir = v3(dir->x - k * normal.x, dir->y - k * normal.y, dir->z - k * normal.z);
+}
+static inline R signr(R a) { return (R)(((R)0 < a) - (a < (R)0)); }   /* math.hh sign */
+static inline void refractive(R index, vec3 normal, vec3 *dir) {   /* refractive.cc:4-22 */
+    vec3 d = *dir;
+    R k = index;
+    R a = dot3(d, normal);
+    if (a < -EPS) k = (R)1 / k;
+    R x = (a * a - (R)1) * (k * k) + (R)1;
+    if (x > EPS) {
+        R b = signr(a) * RSQRT(x);
+        R m = b - a * k;
+        d = v3(d.x * k + m * normal.x, d.y * k + m * normal.y, d.z * k + m * normal.z);
+    } else {
+        R m = (R)2 * a;
+        d = v3(d.x - m * normal.x, d.y - m * normal.y, d.z - m * normal.z);
+    }
+    *dir = d;
+}
+
+/* Emissive<Mixture{Colored<Lambertian>, Specular, Transparent}> (emissive.inl:15-23,
+ * mixture/impl.inl:16-27, colored.inl:15-23, transparent.cc:4-6). */
+static int tl_material_interact(const tl_material *m, uint32_t *rng, vec3 normal, vec3 *dir, col3 *k, col3 *e) {
+    e->x += k->x * m->emission.x;
+    e->y += k->y * m->emission.y;
+    e->z += k->z * m->emission.z;
+    R alpha = rng_uniform(rng);
+    alpha -= m->diffuse;
+    if (alpha < (R)0) {
+        k->x *= m->diffuse_color.x; k->y *= m->diffuse_color.y; k->z *= m->diffuse_color.z;
+        lambertian(rng, normal, dir);
+        return 1;
+    }
+    alpha -= m->specular;
+    if (alpha < (R)0) { specular(normal, dir); return 1; }
+    alpha -= m->transparent;
+    if (alpha < (R)0) return 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ hyperbolic maps
+ * geometry/hyperbolic.cc:40-54 (hy_xshift, hy_zrotate), matrix_complex.cc:38-45 (c22_dot) */
+static inline comp cmake(R x, R y) { comp c = {x, y}; return c; }
+static inline comp c_mul(comp a, comp b) { return cmake(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+static inline comp c_add(comp a, comp b) { return cmake(a.x + b.x, a.y + b.y); }
+static inline moebius mo_chain(moebius a, moebius b) {
+    moebius r;
+    r.a = c_add(c_mul(a.a, b.a), c_mul(a.b, b.c));
+    r.b = c_add(c_mul(a.a, b.b), c_mul(a.b, b.d));
+    r.c = c_add(c_mul(a.c, b.a), c_mul(a.d, b.c));
+    r.d = c_add(c_mul(a.c, b.b), c_mul(a.d, b.d));
+    return r;
+}
+#ifdef HT_REAL_DOUBLE
+#define RCOSH(x) cosh(x)
+#define RSINH(x) sinh(x)
+#define RFLOOR(x) floor(x)
+#else
+#define RCOSH(x) coshf(x)
+#define RSINH(x) sinhf(x)
+#define RFLOOR(x) floorf(x)
+#endif
+static inline moebius hy_xshift(R l) {
+    R l2 = l / (R)2;
+    R c = RCOSH(l2), s = RSINH(l2);
+    moebius m;
+    m.a = cmake(c * (R)1, c * (R)0); m.b = cmake(s * (R)1, s * (R)0);
+    m.c = cmake(s * (R)1, s * (R)0); m.d = cmake(c * (R)1, c * (R)0);
+    return m;
+}
+static inline moebius hy_zrotate(R phi) {
+    R c = RCOS(phi / (R)2), s = RSIN(phi / (R)2);
+    moebius m;
+    m.a = cmake(c, s); m.b = cmake((R)0, (R)0); m.c = cmake((R)0, (R)0); m.d = cmake(c, -s);
+    return m;
+}
+
+/* TiledPlane material choice (object/hy/tiled_plane/impl.inl:48-137): 0 / 1 the cell's
+ * material, 2 the border. */
+static int tiled_plane_cell(const tl_object *t, quat p, int star) {
+    int w = 0;
+    R Q = RSQRT(RCOS(PI_R / 4 + PI_R / 5) / RCOS(PI_R / 4 - PI_R / 5));
+    R T = RSQRT(RCOS(PI_R / 4 + PI_R / 5) * RCOS(PI_R / 4 - PI_R / 5));
+    R S = (RCOS(PI_R / 4) - RSIN(PI_R / 5)) / T;
+    R L = T / RCOS(PI_R / 4);
+    R K = L * (2 * RCOS(PI_R / 5) - 1 / RCOS(PI_R / 5));
+    Q = RLOG((1 + Q) / (1 - Q));
+    S = RLOG((1 + S) / (1 - S));
+    if (p.x < (R)0) { p.x = -p.x; w = !w; }
+    if (p.y < (R)0) { p.y = -p.y; w = !w; }
+    p = mo_apply_q(mo_chain(hy_xshift(-Q), hy_zrotate(-PI_R / 4)), p);
+    int e = 0;
+    for (int j = 0; j < 5; ++j) {
+        int a[3] = {0, 0, 0};
+        for (int i = 0; i < 3 - e; ++i) {
+            R o = 2 * PI_R * (i - 1) / 5;
+            a[i] = dot2(RCOS(o), RSIN(o), p.x, p.y) < L;
+        }
+        a[2] = a[2] || e;
+        int s = a[0] + a[1] + a[2];
+        if (s == 3) {
+            break;
+        } else if (s == 2) {
+            int i = (!a[1]) + 2 * (!a[2]);
+            R o = 2 * PI_R * (i - 1) / 5;
+            p = mo_apply_q(mo_chain(hy_zrotate(-PI_R / 5), mo_chain(hy_xshift(-2 * S), hy_zrotate(-o))), p);
+            e = 1;
+            w = !w;
+        } else {
+            int i = a[0];
+            R o = PI_R * (2 * i - 1) / 5;
+            p = mo_apply_q(mo_chain(hy_xshift(-2 * Q), hy_zrotate(-o)), p);
+            e = 0;
+        }
+    }
+    const R br = t->border_width;
+    int bh = 0;
+    for (int i = 0; i < 5; ++i) {
+        R o = 2 * PI_R * i / 5;
+        R dp = dot2(RCOS(o), RSIN(o), p.x, p.y);
+        bh = bh || (dp > (L - br * p.z));
+        if (star) {
+            R ps = K + dp;
+            w = w ^ (ps < (R)0);
+            bh = bh || (RFABS(ps) < br * p.z);
+        }
+    }
+    if (bh) return 2;
+    return w ? 0 : 1;
+}
+
+#define REM(a, b) ((((a) % (b)) + (b)) % (b))   /* math.hh rem */
+
+/* TiledHorosphere material choice (object/hy/tiled_horosphere/impl.inl:44-95). */
+static const tl_material *tiled_horosphere_material(const tl_object *t, quat p, int hexagonal, int n) {
+    int material_no = 0;
+    int border = 0;
+    R br = t->border_width / t->cell_size;
+    R gx = p.x, gy = p.y;
+    if (!hexagonal) {
+        R vx = gx / t->cell_size, vy = gy / t->cell_size;
+        R kx = RFLOOR(vx), ky = RFLOOR(vy);
+        R fx = vx - kx, fy = vy - ky;
+        if (fx < br || fx > 1 - br || fy < br || fy > 1 - br) {
+            border = 1;
+        } else {
+            int hx = REM((int)kx, 2);
+            int hy = REM((int)ky, 2);
+            material_no = 3 * hy - 2 * hx * hy + hx;
+        }
+    } else {
+        R r3 = RSQRT((R)3);
+        R bxx = 2 / r3, bxy = 0;
+        R byx = -1 / r3, byy = 1;
+        R s = t->cell_size * r3 / 2;
+        R hxf = dot2(bxx, bxy, gx, gy) / s;
+        R hyf = dot2(byx, byy, gx, gy) / s;
+        int hx = (int)RFLOOR((RFLOOR(hxf) - RFLOOR(hyf)) / 3);
+        int hy = (int)RFLOOR((RFLOOR(hxf + hyf) - hx) / 2);
+        R ox = (R)hx * 2 + (R)hy * 1;
+        R oy = (R)hx * -1 + (R)hy * 1;
+        hxf -= ox;
+        hyf -= oy;
+        if (RFABS(hxf - 1) > 1 - br || RFABS(hyf) > 1 - br || RFABS(hxf + hyf - 1) > 1 - br) {
+            border = 1;
+        } else {
+            material_no = 2 * hx + hy;
+        }
+    }
+    if (border) return &t->border;
+    return &t->mats[REM(material_no, n)];
+}
+
+static col3 sample_tl(const ext_scene_t *sc, uint32_t hops, uint32_t *rng, R px, R py, R size, uint32_t flags,
+                      stats_t *st) {
+    R u0 = rng_uniform(rng);
+    R u1 = rng_uniform(rng);
+    R jx = (flags & HTO_JITTER_YX) ? u1 : u0;
+    R jy = (flags & HTO_JITTER_YX) ? u0 : u1;
+    R sx = px + size * (jx - (R)0.5f);
+    R sy = py + size * (jy - (R)0.5f);
+    vec3 ld = normalize3(v3(sx, sy, (R)-1 / sc->fov));
+    quat start = q4((R)0, (R)0, (R)1, (R)0);
+    ray_hy ray;
+    ray.dir = normalize4(mo_deriv_q(sc->cam_mo, start, q4(ld.x, ld.y, ld.z, (R)0)));
+    ray.start = mo_apply_q(sc->cam_mo, start);
+    col3 intensity = {1.0f, 1.0f, 1.0f};
+    col3 emission = {0.0f, 0.0f, 0.0f};
+    uint32_t prev_hash = 0xFFFFFFFFu;
+    st->samples += 1;
+    for (uint32_t i = 0; i < hops; ++i) {
+        st->hops += 1;
+        st->object_tests += sc->n;
+        R min_dist = (R)-1;
+        uint32_t min_index = 0;
+        ray_hy min_local = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        quat min_normal = {0, 0, 0, 0};
+        for (uint32_t k = 0; k < sc->n; ++k) {
+            int repeat = (k == prev_hash);
+            ray_hy local = ray_hy_map(ray, sc->tl[k].inv);
+            quat normal;
+            R dist = sc->tl[k].variant < 2 ? plane_hy_detect(repeat, &normal, &local)
+                                           : horosphere_detect(repeat, &normal, &local);
+            if (dist > -EPS && (min_dist <= -EPS || dist < min_dist)) {
+                min_dist = dist; min_index = k; min_local = local; min_normal = normal;
+            }
+        }
+        if (min_dist > -EPS) {
+            st->hits += 1;
+            const tl_object *t = &sc->tl[min_index];
+            ray_hy hit = ray_hy_map(min_local, t->map);
+            ray_hy loc = ray_hy_map(hit, t->inv);
+            const tl_material *m;
+            if (t->variant < 2) {
+                int c = tiled_plane_cell(t, loc.start, t->variant == 0);
+                m = c == 2 ? &t->border : &t->mats[c];
+            } else {
+                m = tiled_horosphere_material(t, loc.start, t->variant == 2, t->variant == 2 ? 3 : 4);
+            }
+            vec3 d3 = v3(loc.dir.x, loc.dir.y, loc.dir.z);
+            vec3 n3 = v3(min_normal.x, min_normal.y, min_normal.z);
+            int ret = tl_material_interact(m, rng, n3, &d3, &intensity, &emission);
+            loc.dir = q4(d3.x, d3.y, d3.z, (R)0);
+            ray = ray_hy_map(loc, t->map);
+            if (!ret) break;
+            prev_hash = min_index;
+        } else {
+            emission.x += sc->background.x * intensity.x;
+            emission.y += sc->background.y * intensity.y;
+            emission.z += sc->background.z * intensity.z;
+            break;
+        }
+    }
+    return emission;
+}
+
+/* ------------------------------------------------------------------ euclidean extras */
+/* cube_eu_detect (shape/eu/cube.cc:3-65); the reference keeps dist_in / dist_out in float. */
+static inline R cube_nearest(vec3 near, vec3 *n) {
+    int xy = near.x > near.y, yz = near.y > near.z, xz = near.x > near.z;
+    if (xy && xz) { n->x = (R)1; return near.x; }
+    if (yz) { n->y = (R)1; return near.y; }
+    n->z = (R)1;
+    return near.z;
+}
+#ifdef HT_REAL_DOUBLE
+#define RFMIN(a, b) fmin(a, b)
+#define RFMAX(a, b) fmax(a, b)
+#else
+#define RFMIN(a, b) fminf(a, b)
+#define RFMAX(a, b) fmaxf(a, b)
+#endif
+static inline R cube_eu_detect(int repeat, vec3 *normal, ray_eu *ray) {
+    vec3 s = ray->start, d = ray->dir;
+    vec3 inv = v3((R)1 / d.x, (R)1 / d.y, (R)1 / d.z);
+    vec3 vmin = v3(((R)-1 - s.x) * inv.x, ((R)-1 - s.y) * inv.y, ((R)-1 - s.z) * inv.z);
+    vec3 vmax = v3(((R)1 - s.x) * inv.x, ((R)1 - s.y) * inv.y, ((R)1 - s.z) * inv.z);
+    vec3 near = v3(RFMIN(vmin.x, vmax.x), RFMIN(vmin.y, vmax.y), RFMIN(vmin.z, vmax.z));
+    vec3 far = v3(RFMAX(vmin.x, vmax.x), RFMAX(vmin.y, vmax.y), RFMAX(vmin.z, vmax.z));
+    vec3 sg = v3(signr(d.x), signr(d.y), signr(d.z));
+    vec3 nin = v3(0, 0, 0);
+    float din = (float)cube_nearest(near, &nin);
+    nin = v3(nin.x * -sg.x, nin.y * -sg.y, nin.z * -sg.z);
+    vec3 nout = v3(0, 0, 0);
+    float dout = -(float)cube_nearest(v3(-far.x, -far.y, -far.z), &nout);
+    nout = v3(nout.x * sg.x, nout.y * sg.y, nout.z * sg.z);
+    if (din > dout) return (R)-1;
+    R dist = din;
+    vec3 n = nin;
+    R w = 2 * EPS * (R)(2 * repeat - 1);
+    if (dist < w) {
+        dist = dout;
+        n = nout;
+        if (dist < w) return (R)-1;
+    }
+    ray->start = v3(s.x + dist * d.x, s.y + dist * d.y, s.z + dist * d.z);
+    *normal = n;
+    return dist;
+}
+
+/* ray_eu_map with Shift3 (ray_map.inl:15-21, shift.cc:44-59): start + v, normalize(dir). */
+static inline ray_eu ray_shift(ray_eu r, vec3 v) {
+    ray_eu o;
+    o.start = v3(r.start.x + v.x, r.start.y + v.y, r.start.z + v.z);
+    o.dir = normalize3(r.dir);
+    return o;
+}
+
+/* Mixture{Colored<Lambertian>, Specular, Colored<Refractive>} */
+static int gr_material_interact(const gr_object *g, uint32_t *rng, vec3 normal, vec3 *dir, col3 *k) {
+    R alpha = rng_uniform(rng);
+    alpha -= g->diffuse;
+    if (alpha < (R)0) {
+        k->x *= g->diffuse_color.x; k->y *= g->diffuse_color.y; k->z *= g->diffuse_color.z;
+        lambertian(rng, normal, dir);
+        return 1;
+    }
+    alpha -= g->specular;
+    if (alpha < (R)0) { specular(normal, dir); return 1; }
+    alpha -= g->refr;
+    if (alpha < (R)0) {
+        k->x *= g->refr_color.x; k->y *= g->refr_color.y; k->z *= g->refr_color.z;
+        refractive(g->refr_index, normal, dir);
+        return 1;
+    }
+    return 0;
+}
+
+static col3 sample_gr(const ext_scene_t *sc, uint32_t hops, uint32_t *rng, R px, R py, R size, uint32_t flags,
+                      stats_t *st) {
+    R u0 = rng_uniform(rng);
+    R u1 = rng_uniform(rng);
+    R jx = (flags & HTO_JITTER_YX) ? u1 : u0;
+    R jy = (flags & HTO_JITTER_YX) ? u0 : u1;
+    R sx = px + size * (jx - (R)0.5f);
+    R sy = py + size * (jy - (R)0.5f);
+    vec3 ld = normalize3(v3(sx, sy, (R)-1 / sc->fov));
+    ray_eu ray;
+    ray.dir = hom3_apply_dir(sc->cam_hom, ld);
+    ray.start = hom3_apply_pos(sc->cam_hom, v3((R)0, (R)0, (R)0));
+    col3 intensity = {1.0f, 1.0f, 1.0f};
+    col3 emission = {0.0f, 0.0f, 0.0f};
+    uint32_t prev_hash = 0xFFFFFFFFu;
+    st->samples += 1;
+    for (uint32_t i = 0; i < hops; ++i) {
+        st->hops += 1;
+        st->object_tests += sc->n;
+        R min_dist = (R)-1;
+        uint32_t min_index = 0;
+        ray_eu min_local = {{0, 0, 0}, {0, 0, 0}};
+        vec3 min_normal = {0, 0, 0};
+        for (uint32_t k = 0; k < sc->n; ++k) {
+            int repeat = (k == prev_hash);
+            ray_eu local = ray_shift(ray, sc->gr[k].shift_inv);
+            vec3 normal;
+            uint32_t sh = sc->gr[k].shape;
+            R dist = sh == 0 ? plane_eu_detect(repeat, &normal, &local)
+                   : sh == 1 ? sphere_eu_detect(repeat, &normal, &local)
+                             : cube_eu_detect(repeat, &normal, &local);
+            if (dist > -EPS && (min_dist <= -EPS || dist < min_dist)) {
+                min_dist = dist; min_index = k; min_local = local; min_normal = normal;
+            }
+        }
+        if (min_dist > -EPS) {
+            st->hits += 1;
+            const gr_object *g = &sc->gr[min_index];
+            ray_eu hit = ray_shift(min_local, g->shift);
+            ray_eu loc = ray_shift(hit, g->shift_inv);
+            int ret = gr_material_interact(g, rng, min_normal, &loc.dir, &intensity);
+            ray = ray_shift(loc, g->shift);
+            if (!ret) break;
+            prev_hash = min_index;
+        } else {
+            /* GradBg (background/gradient.cc:3-13): all in float */
+            float f = 0.5f * ((float)dot3(ray.dir, sc->grad_dir) + 1.0f);
+            f = f < 0.0f ? 0.0f : f;
+            f = 1.0f < f ? 1.0f : f;
+            f = powf(f, sc->grad_power);
+            float g = 1.0f - f;
+            emission.x += (f * sc->grad_c0.x + g * sc->grad_c1.x) * intensity.x;
+            emission.y += (f * sc->grad_c0.y + g * sc->grad_c1.y) * intensity.y;
+            emission.z += (f * sc->grad_c0.z + g * sc->grad_c1.z) * intensity.z;
+            break;
+        }
+    }
+    return emission;
+}
+
+typedef struct {
+    const ext_scene_t *sc;
+    uint32_t hops, W, H, passes, flags;
+    const uint32_t *pixels;
+    size_t n;
+    float *canvas;
+    uint32_t *seeds;
+    size_t next;
+    pthread_mutex_t lock;
+} ext_job_t;
+
+typedef struct { ext_job_t *job; stats_t st; } ext_worker_t;
+
+static void *ext_worker_main(void *arg) {
+    ext_worker_t *w = (ext_worker_t *)arg;
+    ext_job_t *j = w->job;
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        size_t start = j->next;
+        j->next += 64;
+        pthread_mutex_unlock(&j->lock);
+        if (start >= j->n) break;
+        size_t end = start + 64 < j->n ? start + 64 : j->n;
+        for (size_t i = start; i < end; ++i) {
+            const uint32_t px = j->pixels[i];
+            const uint32_t x = px % j->W, y = px / j->W;
+            const R pxr = ((R)(2u * x + 1u) - (R)j->W) / (R)j->H;
+            const R pyr = ((R)j->H - (R)(2u * y + 1u)) / (R)j->H;
+            const R size = (R)2 / (R)j->H;
+            for (uint32_t p = 0; p < j->passes; ++p) {
+                uint32_t rng = j->seeds[i];
+                col3 c = j->sc->recipe == 3 ? sample_tl(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st)
+                                            : sample_gr(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st);
+                float *cv = j->canvas + 4 * i;
+                cv[0] += c.x; cv[1] += c.y; cv[2] += c.z; cv[3] += 1.0f;
+                j->seeds[i] = rng;
+            }
+        }
+    }
+    return NULL;
+}
+
+static int render_ext(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, int address_width,
+                      uint32_t W, uint32_t H, const uint32_t *pixels, size_t n_pixels, uint32_t passes,
+                      float *canvas, uint32_t *seeds, uint32_t flags, int threads, uint64_t *stats) {
+    if (hops == 0) return -3;
+    if (W == 0 || H == 0) return -1;
+    ext_scene_t sc;
+    int rc = ext_parse(recipe, scene, scene_len, address_width, &sc);
+    if (rc != 0) return rc;
+    if (threads < 1) threads = 1;
+    ext_job_t job;
+    job.sc = &sc; job.hops = hops; job.W = W; job.H = H; job.passes = passes; job.flags = flags;
+    job.pixels = pixels; job.n = n_pixels; job.canvas = canvas; job.seeds = seeds; job.next = 0;
+    pthread_mutex_init(&job.lock, NULL);
+    ext_worker_t *ws = (ext_worker_t *)calloc((size_t)threads, sizeof(ext_worker_t));
+    pthread_t *ts = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int t = 0; t < threads; ++t) ws[t].job = &job;
+    for (int t = 1; t < threads; ++t) pthread_create(&ts[t], NULL, ext_worker_main, &ws[t]);
+    ext_worker_main(&ws[0]);
+    for (int t = 1; t < threads; ++t) pthread_join(ts[t], NULL);
+    if (stats) {
+        stats_t s = {0, 0, 0, 0};
+        for (int t = 0; t < threads; ++t) {
+            s.samples += ws[t].st.samples; s.hops += ws[t].st.hops;
+            s.object_tests += ws[t].st.object_tests; s.hits += ws[t].st.hits;
+        }
+        stats[0] = s.samples; stats[1] = s.hops; stats[2] = s.object_tests; stats[3] = s.hits;
+    }
+    free(ws); free(ts);
+    pthread_mutex_destroy(&job.lock);
+    free(sc.tl); free(sc.gr);
+    return 0;
 }

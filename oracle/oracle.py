@@ -95,7 +95,7 @@ def render(scene_bytes: bytes, recipe: int, hops: int, width: int, height: int,
         if address_width != 32:
             raise ValueError("the reference harness parses X32 scenes")
         lib = _load(os.path.join(REF_DIR, f"libhtref_f{precision}.so"))
-        fn = lib.htref_render
+        fn = lib.htref_render if recipe in (1, 2) else lib.htref_render_ext
         fn.restype = ctypes.c_int
         fn.argtypes = [ctypes.c_int, ctypes.c_uint32, _u8p, ctypes.c_size_t, ctypes.c_uint32,
                        ctypes.c_uint32, _u32p, ctypes.c_size_t, ctypes.c_uint32, _f32p, _u32p,

@@ -18,28 +18,39 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from hypertrace_b200 import scene as S  # noqa: E402
+from hypertrace_b200 import types as T  # noqa: E402
 from oracle import oracle  # noqa: E402
 
+FORCE = "--force" in sys.argv
 
-def render_fixture(name, wl, W, H, n_pixels, passes, seed):
-    sc = wl.scene
+
+def bytes_fixture(name, data, recipe, hops, global_seed, W, H, n_pixels, passes, seed):
+    path = os.path.join(HERE, f"{name}.npz")
+    if os.path.exists(path) and not FORCE:
+        return
     rng = np.random.default_rng(seed)
     pix = np.sort(rng.choice(W * H, n_pixels, replace=False)).astype(np.uint32)
-    seeds = S.pixel_seeds(wl.global_seed, W * H)[pix]
-    data = sc.to_bytes()
-    out = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds, passes=passes, impl="reference", threads=8)
-    out64 = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds, passes=passes, impl="reference",
+    seeds = S.pixel_seeds(global_seed, W * H)[pix]
+    out = oracle.render(data, recipe, hops, W, H, pix, seeds, passes=passes, impl="reference", threads=8)
+    out64 = oracle.render(data, recipe, hops, W, H, pix, seeds, passes=passes, impl="reference",
                           threads=8, precision=64)
     np.savez_compressed(
-        os.path.join(HERE, f"{name}.npz"),
-        scene=np.frombuffer(data, dtype=np.uint8), recipe=sc.recipe, hops=sc.hops, width=W, height=H,
+        path,
+        scene=np.frombuffer(data, dtype=np.uint8), recipe=recipe, hops=hops, width=W, height=H,
         passes=passes, pixels=pix, seeds_in=seeds, canvas_out=out.canvas, seeds_out=out.seeds,
         stats=np.array([out.stats[k] for k in ("samples", "hops", "object_tests", "hits")], dtype=np.uint64),
         canvas_out_f64=out64.canvas, seeds_out_f64=out64.seeds)
     print(name, out.stats)
 
 
+def render_fixture(name, wl, W, H, n_pixels, passes, seed):
+    sc = wl.scene
+    bytes_fixture(name, sc.to_bytes(), sc.recipe, sc.hops, wl.global_seed, W, H, n_pixels, passes, seed)
+
+
 def rng_fixture():
+    if os.path.exists(os.path.join(HERE, "rng_stream.npz")) and not FORCE:
+        return
     vals, state = oracle.rng_uniforms(0xDEADBEEF, 256, impl="reference")
     np.savez_compressed(os.path.join(HERE, "rng_stream.npz"), seed=np.uint32(0xDEADBEEF), uniforms=vals,
                         state=np.uint32(state))
@@ -58,3 +69,8 @@ if __name__ == "__main__":
     one = S.hyperbolic_scene(3, 2, 2.0, 1, 12)
     render_fixture("hyperbolic_onehop", S.Workload("onehop", one, 40, 30, 1, 12), 40, 30, 400, 3, 5)
     render_fixture("euclidean_1px", S.Workload("1px", S.euclidean_scene(4, 4, 13), 1, 1, 1, 13), 1, 1, 1, 4, 6)
+    # the scene types of the reference's hy and eu examples (recipes 3 and 4)
+    bytes_fixture("hy_tiled_800x600", T.serialize(T.hy_tiled_type(), T.hy_example_value()), 3, 3, 0x5EED0005,
+                  800, 600, 800, 3, 7)
+    bytes_fixture("eu_gradient_800x600", T.serialize(T.eu_gradient_type(), T.eu_example_value()), 4, 4, 0x5EED0006,
+                  800, 600, 800, 3, 8)
