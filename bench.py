@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--passes", type=int, default=4, help="passes (samples per pixel) per step")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hy1080", "batched", "serving", "accuracy"], default="hy1080",
+    ap.add_argument("--workload", choices=["hy1080", "batched", "serving", "accuracy", "examples"], default="hy1080",
                     help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views in one "
                          "launch per step; serving: Poisson requests through the continuous-batching server")
     ap.add_argument("--spp-scale", type=float, default=0.25, help="batched: scale of every view's spp")
@@ -208,6 +208,8 @@ def main():
         return bench_batched(args)
     if args.workload == "serving":
         return bench_serving(args)
+    if args.workload == "examples":
+        return bench_examples(args)
     if args.workload == "accuracy":
         return bench_accuracy(args)
     if world > 1:
@@ -469,6 +471,67 @@ def bench_serving(args):
                        "interactive": "1280x720 x 8 spp hyperbolic, moving camera", "batch_spp_scale": 0.125},
             "rates": out}
     print(json.dumps(line), flush=True)
+
+
+def bench_examples(args):
+    """The generic scene programs on the scene types of the reference's hy and eu examples
+    (main/examples/hy.rs: tiled planes and horospheres, transparent material, H = 3;
+    main/examples/eu.rs: plane / sphere / cube, refractive material, gradient background,
+    H = 4) and on a heavier random scene of the hy type: built-in recipe and the same type
+    compiled at run time with NVRTC, each against the reference's own kernel code on the host
+    cores (oracle/_ref, all threads, a bounded pixel sample)."""
+    import torch
+    from hypertrace_b200 import _lib
+    from hypertrace_b200 import processing as P
+    from hypertrace_b200 import scene as S
+    from hypertrace_b200 import types as T
+    from oracle import oracle
+    ctx = P.Context(0)
+    stream = torch.cuda.current_stream(ctx.device)
+    cores = os.cpu_count() or 1
+    cases = [("hy-tiled-example-800x600-h3", T.hy_tiled_type(), T.hy_example_value(), _lib.HTC_RECIPE_HY_TILED, 3, 800, 600),
+             ("eu-gradient-example-800x600-h4", T.eu_gradient_type(), T.eu_example_value(), _lib.HTC_RECIPE_EU_GRADIENT,
+              4, 800, 600),
+             ("hy-tiled-random-1920x1080-64obj-h8", T.hy_tiled_type(), T.hy_tiled_random_value(17, 64, 3.0),
+              _lib.HTC_RECIPE_HY_TILED, 8, 1920, 1080)]
+    results = {}
+    passes = 16
+    for name, ty, val, recipe, hops, W, H in cases:
+        data = T.serialize(ty, val)
+        buf = P.EntityBuffer(ctx, data)
+        res = {}
+        for kind, render in (("builtin", P.Render(ctx, recipe, hops)), ("nvrtc", P.Render.build(ctx, ty, hops))):
+            canvas = P.Canvas(ctx, (W, H), global_seed=0x5EED0007)
+            stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+            for _ in range(max(args.warmup, 1)):
+                render.render_passes(buf, canvas, passes, sync=False)
+            torch.cuda.synchronize()
+            stats.zero_()
+            ms = 0.0
+            for _ in range(args.steps):
+                ms += _time_ms(lambda: render.render_passes(buf, canvas, passes, stats=stats, sync=False), stream)
+            render._check(True)
+            st = stats.cpu().numpy().astype(np.float64)
+            res[kind] = {"Msamples_per_s": st[0] / ms / 1e3, "ray_bounces_per_s": st[1] / ms * 1e3,
+                         "ms_per_step": ms / args.steps, "object_tests_per_hop": st[2] / max(st[1], 1)}
+        cpu = None
+        if oracle.ref_available():
+            rng = np.random.default_rng(3)
+            n = 4096 if W * H > 4096 else W * H
+            pix = np.sort(rng.choice(W * H, n, replace=False)).astype(np.uint32)
+            seeds = S.pixel_seeds(1, W * H)[pix]
+            t0 = time.perf_counter()
+            oracle.render(data, recipe, hops, W, H, pix, seeds, passes=2, impl="reference", threads=cores)
+            dt = time.perf_counter() - t0
+            cpu = {"Msamples_per_s": n * 2 / dt / 1e6, "cores": cores, "kind": "reference",
+                   "sample": f"{n} random pixels x 2 passes"}
+        res["cpu_reference"] = cpu
+        if cpu:
+            res["speedup_builtin_vs_cpu"] = res["builtin"]["Msamples_per_s"] / cpu["Msamples_per_s"]
+        results[name] = res
+    print(json.dumps({"metric": "Msamples/s, generic scene programs (reference example scene types)",
+                      "unit": UNIT, "passes_per_step": passes, "steps": args.steps, "data": "synthetic",
+                      "results": results}), flush=True)
 
 
 def bench_accuracy(args):

@@ -42,10 +42,19 @@ class Context:
 
 
 class EntityBuffer:
-    """Serialized scene bytes on the device (processing/src/buffer.rs:13-29)."""
+    """Serialized scene bytes on the device (processing/src/buffer.rs:13-29).
 
-    def __init__(self, context: Context, scene: Scene):
-        data = serialize(scene, context.config.address_width)
+    `scene` is a scene.Scene (recipes HTC_RECIPE_HY / EU), already serialized bytes, or a
+    value of `scene_type` (a hypertrace_b200.types entity type, for any other scene)."""
+
+    def __init__(self, context: Context, scene, scene_type=None):
+        if isinstance(scene, (bytes, bytearray)):
+            data = bytes(scene)
+        elif scene_type is not None:
+            from . import types as T
+            data = T.serialize(scene_type, scene, context.config.address_width)
+        else:
+            data = serialize(scene, context.config.address_width)
         host = torch.frombuffer(bytearray(data), dtype=torch.uint8).pin_memory()
         self.tensor = host.to(context.device, non_blocking=True)   # ordered on the current stream
         self.size = len(data)
@@ -99,6 +108,30 @@ class Render:
         _lib.call("htc_program_create", recipe, hops, context.config.address_width,
                   int(context.config.double_support), flags, ctypes.byref(handle))
         self.handle = handle
+
+    @classmethod
+    def build(cls, context: Context, scene_type, hops: int, flags: int = 0) -> "Render":
+        """Render::new for any scene type: `scene_type` is a hypertrace_b200.types entity
+        type (or its C++ type expression), compiled at run time with NVRTC
+        (htc_program_build). Raises HtcError with the compiler log on failure."""
+        expr = scene_type if isinstance(scene_type, str) else scene_type.cxx()
+        self = cls.__new__(cls)
+        self.context = context
+        self.recipe = _lib.HTC_RECIPE_CUSTOM
+        self.hops = hops
+        handle = ctypes.c_void_p()
+        log = ctypes.create_string_buffer(1 << 16)
+        rc = _lib.lib().htc_program_build(expr.encode(), hops, context.config.address_width, flags, log,
+                                          len(log), ctypes.byref(handle))
+        self.log = log.value.decode(errors="replace")
+        self.handle = handle
+        _lib.check(rc)
+        return self
+
+    def static_size(self) -> int:
+        v = ctypes.c_uint64()
+        _lib.call("htc_program_static_size", self.handle, ctypes.byref(v))
+        return v.value
 
     def __del__(self):
         h = getattr(self, "handle", None)
