@@ -299,7 +299,7 @@ template <class G, class V, class M> struct MappedView {   // Mapped{phantom, ma
 // starts at the hit point.
 struct PlaneHy {   // shape/hy/plane.cc:4-37
     template <int W> __host__ __device__ static constexpr Lay lay() { return Lay{0u, 1u}; }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, Q4 &normal, Light<Hy> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, Q4 &normal, Light<Hy> &l) {
         if (is_repeat(c)) return -1.0f;
         const Q4 p = l.p, d = l.v;
         const float pd = dot4(p, d);
@@ -311,15 +311,17 @@ struct PlaneHy {   // shape/hy/plane.cc:4-37
         const float pxy2 = dot2(hx, hy, hx, hy);
         if (pxy2 > 1.0f) return -1.0f;
         const Q4 h = q4(hx, hy, sqrtf(1.0f - pxy2), 0.0f);
-        l.p = h;
-        l.v = hy_dir_at(p, d, h);
-        normal = q4(-h.x, -h.y, -h.z, -h.w);
+        if (F) {
+            l.p = h;
+            l.v = hy_dir_at(p, d, h);
+            normal = q4(-h.x, -h.y, -h.z, -h.w);
+        }
         return hy_distance(p, h);
     }
 };
 struct Horosphere {   // shape/hy/horosphere.cc:4-34
     template <int W> __host__ __device__ static constexpr Lay lay() { return Lay{0u, 1u}; }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, Q4 &normal, Light<Hy> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, Q4 &normal, Light<Hy> &l) {
         const bool repeat = is_repeat(c);
         const Q4 p = l.p, d = l.v;
         const float dxy = sqrtf(dot2(d.x, d.y, d.x, d.y));
@@ -333,15 +335,17 @@ struct Horosphere {   // shape/hy/horosphere.cc:4-34
         }
         t /= dxy * dxy;
         const Q4 h = q4(p.x + d.x * t, p.y + d.y * t, 1.0f, 0.0f);
-        l.p = h;
-        l.v = hy_dir_at(p, d, h);
-        normal = q4(0.0f, 0.0f, -1.0f, 0.0f);
+        if (F) {
+            l.p = h;
+            l.v = hy_dir_at(p, d, h);
+            normal = q4(0.0f, 0.0f, -1.0f, 0.0f);
+        }
         return hy_distance(p, h);
     }
 };
 struct PlaneEu {   // shape/eu/plane.cc:3-21
     template <int W> __host__ __device__ static constexpr Lay lay() { return Lay{0u, 1u}; }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
         if (is_repeat(c)) return -1.0f;
         const V3 pos = l.p, dir = l.v;
         if (pos.z * dir.z > 0.0f) return -1.0f;
@@ -353,7 +357,7 @@ struct PlaneEu {   // shape/eu/plane.cc:3-21
 };
 struct Sphere {   // shape/eu/sphere.cc:3-29
     template <int W> __host__ __device__ static constexpr Lay lay() { return Lay{0u, 1u}; }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
         const bool repeat = is_repeat(c);
         const V3 pos = l.p, dir = l.v;
         const float b = -dot3(dir, pos);
@@ -367,9 +371,11 @@ struct Sphere {   // shape/eu/sphere.cc:3-29
             e = b + d;
             if (e < w) return -1.0f;
         }
-        const V3 h = normalize3(v3(pos.x + dir.x * e, pos.y + dir.y * e, pos.z + dir.z * e));
-        normal = h;
-        l.p = h;
+        if (F) {
+            const V3 h = normalize3(v3(pos.x + dir.x * e, pos.y + dir.y * e, pos.z + dir.z * e));
+            normal = h;
+            l.p = h;
+        }
         return e;
     }
 };
@@ -383,7 +389,7 @@ struct Cube {   // shape/eu/cube.cc:3-65
         n.z = 1.0f;
         return near.z;
     }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, V3 &normal, Light<Eu> &l) {
         const bool repeat = is_repeat(c);
         const V3 s = l.p, d = l.v;
         const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -416,57 +422,63 @@ template <class G, class S> struct ShapeVec {   // shape/vector.inl
     template <int W> __host__ __device__ static constexpr Lay lay() {
         return Lay{upm((u32)W, S::template lay<W>().align), lcmc((u32)W, S::template lay<W>().align)};
     }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &normal, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &normal, Light<G> &l) {
         constexpr u32 stride = S::template lay<W>().size;
         constexpr u32 head = upm((u32)W, S::template lay<W>().align);
         u32 n = ldusize<W>(self);
         if (stride > 0 && (c.end < self + head || n > (u32)((c.end - self - head) / stride))) { atomicOr(c.err, ERR_SCENE); n = 0; }
+        // Distances first, then the winner's full detection again (same operations, same
+        // bits) instead of keeping every candidate's light and normal (shape/vector.inl).
         const u32 orig = c.hasher;
         float min_dist = -1.0f;
-        typename G::Dir min_normal = normal;
-        Light<G> min_light = l;
-        u32 min_hasher = orig;
+        u32 min_index = 0, min_hasher = orig;
         for (u32 i = 0; i < n; ++i) {
             Light<G> cur = l;
             typename G::Dir cn;
             hash_usize(c, i);
-            const float dist = S::template detect<W>(self + head + i * stride, c, cn, cur);
+            const float dist = S::template detect<W, false>(self + head + i * stride, c, cn, cur);
             if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
-                min_dist = dist; min_normal = cn; min_light = cur; min_hasher = c.hasher;
+                min_dist = dist; min_index = i; min_hasher = c.hasher;
             }
             c.hasher = orig;
         }
-        if (min_dist > -EPSF) {
-            normal = min_normal; l = min_light; c.hasher = min_hasher;
-            return min_dist;
+        if (!(min_dist > -EPSF)) return -1.0f;
+        if (F) {
+            const u32 tests = c.tests;
+            hash_usize(c, min_index);
+            S::template detect<W, true>(self + head + min_index * stride, c, normal, l);
+            c.tests = tests;
         }
-        return -1.0f;
+        c.hasher = min_hasher;
+        return min_dist;
     }
 };
 template <class G, class S, class M> struct MappedShape {   // shape/mapped.inl
     typedef Rec<4, Zst, M, S> R4;
     template <int W> __host__ __device__ static constexpr Lay lay() { return Rec<W, Zst, M, S>::lay(); }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &normal, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &normal, Light<G> &l) {
         const typename M::V m = M::load(self + Rec<W, Zst, M, S>::off(1));
         MapOps<M>::ray(M::inverse(m), l.p, l.v);
-        const float dist = S::template detect<W>(self + Rec<W, Zst, M, S>::off(2), c, normal, l);
-        normal = M::normal(m, l.p, normal);
-        MapOps<M>::ray(m, l.p, l.v);
+        const float dist = S::template detect<W, F>(self + Rec<W, Zst, M, S>::off(2), c, normal, l);
+        if (F) {
+            normal = M::normal(m, l.p, normal);
+            MapOps<M>::ray(m, l.p, l.v);
+        }
         return dist;
     }
 };
 template <class G, class... S> struct ShapeChoice;   // shape/choice/impl.inl
 template <class G> struct ShapeChoice<G> {
-    template <int W> HT_D static float dispatch(u32, Ptr, Ctx &, typename G::Dir &, Light<G> &) { return -1.0f; }
+    template <int W, bool F> HT_D static float dispatch(u32, Ptr, Ctx &, typename G::Dir &, Light<G> &) { return -1.0f; }
 };
 template <class G, class S0, class... S> struct ShapeChoice<G, S0, S...> {
     template <int W> __host__ __device__ static constexpr Lay lay() { return Enum<W, S0, S...>::lay(); }
-    template <int W> HT_D static float dispatch(u32 i, Ptr pay, Ctx &c, typename G::Dir &n, Light<G> &l) {
-        if (i == 0) return S0::template detect<W>(pay, c, n, l);
-        return ShapeChoice<G, S...>::template dispatch<W>(i - 1, pay, c, n, l);
+    template <int W, bool F> HT_D static float dispatch(u32 i, Ptr pay, Ctx &c, typename G::Dir &n, Light<G> &l) {
+        if (i == 0) return S0::template detect<W, F>(pay, c, n, l);
+        return ShapeChoice<G, S...>::template dispatch<W, F>(i - 1, pay, c, n, l);
     }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &n, Light<G> &l) {
-        return dispatch<W>(ldusize<W>(self), self + Enum<W, S0, S...>::payload(), c, n, l);
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &n, Light<G> &l) {
+        return dispatch<W, F>(ldusize<W>(self), self + Enum<W, S0, S...>::payload(), c, n, l);
     }
 };
 
@@ -590,9 +602,9 @@ template <class G> struct NormalCache { typename G::Dir normal; };
 template <class G, class S, class M> struct Covered {   // {material, shape} (object/covered.rs:12-18)
     typedef NormalCache<G> Cache;
     template <int W> __host__ __device__ static constexpr Lay lay() { return Rec<W, Zst, M, S>::lay(); }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
         ++c.tests;
-        return S::template detect<W>(self + Rec<W, Zst, M, S>::off(2), c, cache.normal, l);
+        return S::template detect<W, F>(self + Rec<W, Zst, M, S>::off(2), c, cache.normal, l);
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<G> &l, Col &e) {
         LightLocal ll;   // light_<geo>_to_local
@@ -607,11 +619,11 @@ template <class G, class S, class M> struct Covered {   // {material, shape} (ob
 template <class G, class O, class M> struct MappedObject {   // object/mapped.inl
     typedef typename O::Cache Cache;
     template <int W> __host__ __device__ static constexpr Lay lay() { return Rec<W, Zst, M, O>::lay(); }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
         const typename M::V m = M::load(self + Rec<W, Zst, M, O>::off(1));
         MapOps<M>::ray(M::inverse(m), l.p, l.v);
-        const float dist = O::template detect<W>(self + Rec<W, Zst, M, O>::off(2), c, cache, l);
-        MapOps<M>::ray(m, l.p, l.v);
+        const float dist = O::template detect<W, F>(self + Rec<W, Zst, M, O>::off(2), c, cache, l);
+        if (F) MapOps<M>::ray(m, l.p, l.v);
         return dist;
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<G> &l, Col &e) {
@@ -634,30 +646,37 @@ template <class G, class O> struct ObjectVec {   // object/vector.inl
         if (stride > 0 && (c.end < self + head || n > (u32)((c.end - self - head) / stride))) { atomicOr(c.err, ERR_SCENE); n = 0; }
         return n;
     }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
         constexpr u32 stride = O::template lay<W>().size;
         constexpr u32 head = upm((u32)W, O::template lay<W>().align);
+        // Distances first (no map back, no hit direction), then the winner's full detection
+        // again: the same operations give the same bits as keeping every candidate's light
+        // and cache (object/vector.inl:24-62), for one map back per hop instead of one per
+        // candidate.
         const u32 n = count<W>(self, c);
         const u32 orig = c.hasher;
         float min_dist = -1.0f;
         u32 min_index = 0, min_hasher = orig;
-        Light<G> min_light = l;
-        typename O::Cache min_cache;
         for (u32 i = 0; i < n; ++i) {
             Light<G> cur = l;
             typename O::Cache cc;
             hash_usize(c, i);
-            const float dist = O::template detect<W>(self + head + i * stride, c, cc, cur);
+            const float dist = O::template detect<W, false>(self + head + i * stride, c, cc, cur);
             if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
-                min_dist = dist; min_index = i; min_light = cur; min_cache = cc; min_hasher = c.hasher;
+                min_dist = dist; min_index = i; min_hasher = c.hasher;
             }
             c.hasher = orig;
         }
-        if (min_dist > -EPSF) {
-            cache.inner = min_cache; cache.index = min_index; l = min_light; c.hasher = min_hasher;
-            return min_dist;
+        if (!(min_dist > -EPSF)) return -1.0f;
+        if (F) {
+            const u32 tests = c.tests;
+            hash_usize(c, min_index);
+            O::template detect<W, true>(self + head + min_index * stride, c, cache.inner, l);
+            c.tests = tests;
+            cache.index = min_index;
         }
-        return -1.0f;
+        c.hasher = min_hasher;
+        return min_dist;
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<G> &l, Col &e) {
         constexpr u32 stride = O::template lay<W>().size;
@@ -672,13 +691,13 @@ template <> struct CacheTuple<> {};
 template <class O0, class... O> struct CacheTuple<O0, O...> { typename O0::Cache head; CacheTuple<O...> tail; };
 template <class G, class... O> struct ObjectChoiceImpl;
 template <class G> struct ObjectChoiceImpl<G> {
-    template <int W> HT_D static float detect(u32, Ptr, Ctx &, CacheTuple<> &, Light<G> &) { return -1.0f; }
+    template <int W, bool F = true> HT_D static float detect(u32, Ptr, Ctx &, CacheTuple<> &, Light<G> &) { return -1.0f; }
     template <int W> HT_D static bool interact(u32, Ptr, Ctx &, CacheTuple<> &, Light<G> &, Col &) { return false; }
 };
 template <class G, class O0, class... O> struct ObjectChoiceImpl<G, O0, O...> {
-    template <int W> HT_D static float detect(u32 i, Ptr pay, Ctx &c, CacheTuple<O0, O...> &cache, Light<G> &l) {
-        if (i == 0) return O0::template detect<W>(pay, c, cache.head, l);
-        return ObjectChoiceImpl<G, O...>::template detect<W>(i - 1, pay, c, cache.tail, l);
+    template <int W, bool F = true> HT_D static float detect(u32 i, Ptr pay, Ctx &c, CacheTuple<O0, O...> &cache, Light<G> &l) {
+        if (i == 0) return O0::template detect<W, F>(pay, c, cache.head, l);
+        return ObjectChoiceImpl<G, O...>::template detect<W, F>(i - 1, pay, c, cache.tail, l);
     }
     template <int W> HT_D static bool interact(u32 i, Ptr pay, Ctx &c, CacheTuple<O0, O...> &cache, Light<G> &l, Col &e) {
         if (i == 0) return O0::template interact<W>(pay, c, cache.head, l, e);
@@ -688,8 +707,8 @@ template <class G, class O0, class... O> struct ObjectChoiceImpl<G, O0, O...> {
 template <class G, class... O> struct ObjectChoice {   // object/choice/impl.inl
     typedef CacheTuple<O...> Cache;
     template <int W> __host__ __device__ static constexpr Lay lay() { return Enum<W, O...>::lay(); }
-    template <int W> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
-        return ObjectChoiceImpl<G, O...>::template detect<W>(ldusize<W>(self), self + Enum<W, O...>::payload(), c, cache, l);
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+        return ObjectChoiceImpl<G, O...>::template detect<W, F>(ldusize<W>(self), self + Enum<W, O...>::payload(), c, cache, l);
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<G> &l, Col &e) {
         return ObjectChoiceImpl<G, O...>::template interact<W>(ldusize<W>(self), self + Enum<W, O...>::payload(), c, cache, l, e);
@@ -793,9 +812,9 @@ template <class M, class K, int N> struct TiledPlane {   // object/hy/tiled_plan
     typedef NormalCache<Hy> Cache;
     template <int W> using R = typename TiledFields<M, K, N>::template R<W>;
     template <int W> __host__ __device__ static constexpr Lay lay() { return R<W>::lay(); }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, Cache &cache, Light<Hy> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, Cache &cache, Light<Hy> &l) {
         ++c.tests;
-        return PlaneHy::detect<W>(nullptr, c, cache.normal, l);
+        return PlaneHy::detect<W, F>(nullptr, c, cache.normal, l);
     }
     template <int W> HT_D static u32 cell(Ptr self, Q4 p) {   // 0 / 1: materials, 2: border
         const PentaTables &t = g_penta;
@@ -864,9 +883,9 @@ template <class M, class K, int N> struct TiledHorosphere {   // object/hy/tiled
     typedef NormalCache<Hy> Cache;
     template <int W> using R = typename TiledFields<M, K, N>::template R<W>;
     template <int W> __host__ __device__ static constexpr Lay lay() { return R<W>::lay(); }
-    template <int W> HT_D static float detect(Ptr, Ctx &c, Cache &cache, Light<Hy> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr, Ctx &c, Cache &cache, Light<Hy> &l) {
         ++c.tests;
-        return Horosphere::detect<W>(nullptr, c, cache.normal, l);
+        return Horosphere::detect<W, F>(nullptr, c, cache.normal, l);
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<Hy> &l, Col &e) {
         int material_no = 0;
@@ -924,7 +943,7 @@ template <class G, class V, class O, class B> struct SceneImpl {   // {phantom, 
             c.hasher = 0u;
             typename O::Cache cache;
             ++hops_done;
-            const float dist = O::template detect<W>(self + R<W>::off(3), c, cache, l);
+            const float dist = O::template detect<W, true>(self + R<W>::off(3), c, cache, l);
             if (dist > -0.5f) {
                 ++hits;
                 const bool ret = O::template interact<W>(self + R<W>::off(3), c, cache, l, e);
