@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--case", type=str, default="", help="examples: run only the cases whose name contains this")
     return ap.parse_args()
 
 
@@ -496,6 +497,7 @@ def bench_examples(args):
               _lib.HTC_RECIPE_HY_TILED, 8, 1920, 1080)]
     results = {}
     passes = 16
+    cases = [c for c in cases if args.case in c[0]]
     for name, ty, val, recipe, hops, W, H in cases:
         data = T.serialize(ty, val)
         buf = P.EntityBuffer(ctx, data)

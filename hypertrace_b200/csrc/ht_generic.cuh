@@ -961,8 +961,14 @@ template <class G, class V, class O, class B> struct SceneImpl {   // {phantom, 
 // ============================================================================ kernel
 // One thread per pixel (render/render.cl:6-27); `passes` samples of the pixel in order, the
 // same float additions as `passes` launches of one pass.
+// Resident 128-thread blocks per SM requested from ptxas (register cap 64): the scan is a
+// chain of dependent FP32 operations, so more resident warps beat the few spilled values
+// (8 blocks measured fastest against 1, 5, 6, 7 on the example scene types).
+#ifndef HTG_MIN_BLOCKS
+#define HTG_MIN_BLOCKS 8
+#endif
 template <class Scene, int W>
-__global__ void __launch_bounds__(128) render_generic(Ptr scene, uint64_t scene_size, u32 width, u32 height,
+__global__ void __launch_bounds__(128, HTG_MIN_BLOCKS) render_generic(Ptr scene, uint64_t scene_size, u32 width, u32 height,
                                                      u32 hops, u32 passes, u32 flags, float4 *canvas, u32 *seeds,
                                                      unsigned long long *stats, u32 *err) {
     const u32 idx = blockIdx.x * 128u + threadIdx.x;
