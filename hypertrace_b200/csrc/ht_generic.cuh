@@ -259,11 +259,15 @@ template <class M> struct EuMapOps {
         v = M::dir(m, p, v);
         p = M::pos(m, p);
     }
+    HT_D static void ray_cold(const typename M::V &m, V3 &p, V3 &v) { ray(m, p, v); }
 };
 template <class M> struct MapOps : EuMapOps<M> {};
 template <> struct MapOps<Moebius> {
     HT_D static void ray(const Mo &m, Q4 &p, Q4 &v) { Moebius::ray(m, p, v); }
     HT_D static void view(const Mo &m, Q4 &p, Q4 &v) { Moebius::view(m, p, v); }
+    // The same map through one out-of-line copy, for the once-per-hop paths (the winner's
+    // full detection, the interaction): only the distance scan keeps an inlined copy.
+    HT_D static void ray_cold(const Mo &m, Q4 &p, Q4 &v) { HyRay r = ray_hy_map_call(m, p, v); p = r.p; v = r.v; }
 };
 
 // ============================================================================ views
@@ -458,11 +462,12 @@ template <class G, class S, class M> struct MappedShape {   // shape/mapped.inl
     template <int W> __host__ __device__ static constexpr Lay lay() { return Rec<W, Zst, M, S>::lay(); }
     template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, typename G::Dir &normal, Light<G> &l) {
         const typename M::V m = M::load(self + Rec<W, Zst, M, S>::off(1));
-        MapOps<M>::ray(M::inverse(m), l.p, l.v);
+        if (F) MapOps<M>::ray_cold(M::inverse(m), l.p, l.v);
+        else MapOps<M>::ray(M::inverse(m), l.p, l.v);
         const float dist = S::template detect<W, F>(self + Rec<W, Zst, M, S>::off(2), c, normal, l);
         if (F) {
             normal = M::normal(m, l.p, normal);
-            MapOps<M>::ray(m, l.p, l.v);
+            MapOps<M>::ray_cold(m, l.p, l.v);
         }
         return dist;
     }
@@ -630,16 +635,17 @@ template <class G, class O, class M> struct MappedObject {   // object/mapped.in
     template <int W> __host__ __device__ static constexpr Lay lay() { return Rec<W, Zst, M, O>::lay(); }
     template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
         const typename M::V m = M::load(self + Rec<W, Zst, M, O>::off(1));
-        MapOps<M>::ray(M::inverse(m), l.p, l.v);
+        if (F) MapOps<M>::ray_cold(M::inverse(m), l.p, l.v);
+        else MapOps<M>::ray(M::inverse(m), l.p, l.v);
         const float dist = O::template detect<W, F>(self + Rec<W, Zst, M, O>::off(2), c, cache, l);
-        if (F) MapOps<M>::ray(m, l.p, l.v);
+        if (F) MapOps<M>::ray_cold(m, l.p, l.v);
         return dist;
     }
     template <int W> HT_D static bool interact(Ptr self, Ctx &c, Cache &cache, Light<G> &l, Col &e) {
         const typename M::V m = M::load(self + Rec<W, Zst, M, O>::off(1));
-        MapOps<M>::ray(M::inverse(m), l.p, l.v);
+        MapOps<M>::ray_cold(M::inverse(m), l.p, l.v);
         const bool ret = O::template interact<W>(self + Rec<W, Zst, M, O>::off(2), c, cache, l, e);
-        MapOps<M>::ray(m, l.p, l.v);
+        MapOps<M>::ray_cold(m, l.p, l.v);
         return ret;
     }
 };
