@@ -16,7 +16,8 @@
 //
 // Entities (reference files):
 //   maps        Moebius (transform/moebius.cc), Shift3 (shift.cc), Rotation3 (rotation.cc),
-//               Chain<A, B> (chain.inl; Homogenous3 = Chain<Shift3, Rotation3>)
+//               Linear3 (linear.cc), Chain<A, B> of Shift3 with Rotation3 or Linear3 in either
+//               order (chain.inl; Homogenous3 = Chain<Shift3, Rotation3>)
 //   views       PointView<G> (view/point/impl.inl), MappedView<G, V, M> (view/mapped.inl)
 //   shapes      PlaneHy, Horosphere (shape/hy/*.cc), PlaneEu, Sphere, Cube (shape/eu/*.cc),
 //               ShapeVec<G, S> (shape/vector.inl), MappedShape<G, S, M> (shape/mapped.inl),
@@ -214,13 +215,68 @@ struct Rotation3 {
     HT_D static V3 dir(const V &m, V3, V3 d) { return rot3_apply(m, d); }
     HT_D static V3 normal(const V &m, V3, V3 d) { return rot3_apply(m, d); }
 };
-// <inner>_<outer>_reorder (rotation.cc: rot3_shf3_reorder, shf3_rot3_reorder)
+// Linear3: a 3x3 matrix stored as a 4x4 real16, rows (m0 m1 m2 0), (m4 m5 m6 0),
+// (m8 m9 m10 0), (0 0 0 1) (types/src/primitive/matrix.rs:117-165; transform/linear.cc,
+// algebra/matrix_real.cc).
+struct M33 { float m[16]; };
+HT_D V3 r33_dot_mv(const M33 &a, V3 b) {   // r44_dot_mv(a, (b, 0)).xyz: dot of 4-vectors from 0
+    V3 r;
+    float c;
+    c = 0.0f; c += a.m[0] * b.x; c += a.m[1] * b.y; c += a.m[2] * b.z; c += a.m[3] * 0.0f; r.x = c;
+    c = 0.0f; c += a.m[4] * b.x; c += a.m[5] * b.y; c += a.m[6] * b.z; c += a.m[7] * 0.0f; r.y = c;
+    c = 0.0f; c += a.m[8] * b.x; c += a.m[9] * b.y; c += a.m[10] * b.z; c += a.m[11] * 0.0f; r.z = c;
+    return r;
+}
+HT_D M33 r33_transpose(const M33 &a) {
+    M33 t;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) t.m[4 * i + j] = a.m[4 * j + i];
+    return t;
+}
+HT_D M33 r33_inverse(const M33 &a) {   // matrix_real.cc:106-120: adjugate / det, then s_f = 1
+    const float *m = a.m;
+    const float det = m[0] * m[5] * m[10] + m[1] * m[6] * m[8] + m[2] * m[4] * m[9]
+                    - m[0] * m[6] * m[9] - m[1] * m[4] * m[10] - m[2] * m[5] * m[8];
+    const float adj[16] = {m[5] * m[10] - m[6] * m[9], m[2] * m[9] - m[1] * m[10], m[1] * m[6] - m[2] * m[5], 0.0f,
+                           m[6] * m[8] - m[4] * m[10], m[0] * m[10] - m[2] * m[8], m[2] * m[4] - m[0] * m[6], 0.0f,
+                           m[4] * m[9] - m[5] * m[8], m[1] * m[8] - m[0] * m[9], m[0] * m[5] - m[1] * m[4], 0.0f,
+                           0.0f, 0.0f, 0.0f, 0.0f};
+    M33 r;
+    for (int i = 0; i < 16; ++i) r.m[i] = adj[i] / det;
+    r.m[15] = 1.0f;
+    return r;
+}
+struct Linear3 {
+    typedef M33 V;
+    template <int W> __host__ __device__ static constexpr Lay lay() { return Lay{64u, 64u}; }
+    HT_D static V load(Ptr p) {
+        M33 m;
+        for (int i = 0; i < 4; ++i) {
+            const float4 r = __ldg(reinterpret_cast<const float4 *>(p + 16 * i));
+            m.m[4 * i] = r.x; m.m[4 * i + 1] = r.y; m.m[4 * i + 2] = r.z; m.m[4 * i + 3] = r.w;
+        }
+        return m;
+    }
+    HT_D static V inverse(const V &m) { return r33_inverse(m); }
+    HT_D static V3 pos(const V &m, V3 p) { return r33_dot_mv(m, p); }
+    HT_D static V3 dir(const V &m, V3, V3 d) { return normalize3(r33_dot_mv(m, d)); }
+    HT_D static V3 normal(const V &m, V3, V3 d) { return normalize3(r33_dot_mv(r33_transpose(r33_inverse(m)), d)); }
+};
+
+// <inner>_<outer>_reorder (rotation.cc: rot3_shf3_reorder, shf3_rot3_reorder;
+// linear.cc: lin3_shf3_reorder, shf3_lin3_reorder)
 template <class Inner, class Outer> struct Reorder;
 template <> struct Reorder<Rotation3, Shift3> {
     HT_D static void apply(Q4 &inner, V3 &outer) { outer = rot3_apply(inner, outer); }
 };
 template <> struct Reorder<Shift3, Rotation3> {
     HT_D static void apply(V3 &inner, Q4 &outer) { inner = rot3_apply(q_conj(outer), inner); }
+};
+template <> struct Reorder<Linear3, Shift3> {
+    HT_D static void apply(M33 &inner, V3 &outer) { outer = r33_dot_mv(inner, outer); }
+};
+template <> struct Reorder<Shift3, Linear3> {
+    HT_D static void apply(V3 &inner, M33 &outer) { inner = r33_dot_mv(r33_inverse(outer), inner); }
 };
 template <class A, class B> struct Chain {   // outer A after inner B (transform/chain.inl)
     struct V { typename A::V a; typename B::V b; };

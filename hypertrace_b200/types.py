@@ -303,6 +303,24 @@ class Rotation3(Entity):
         Quat().write(buf, off, value, W)
 
 
+class Linear3(Entity):
+    """Linear<f64, 3> as real3x3 = 16 floats, rows padded with 0 and a last row (0, 0, 0, 1)
+    (types/src/primitive/matrix.rs:117-165); value: a 3x3 array."""
+    geo = "Eu"
+
+    def cxx(self):
+        return "Linear3"
+
+    def lay(self, W):
+        return (64, 64)
+
+    def write(self, buf, off, value, W):
+        m = np.asarray(value, dtype=np.float64).reshape(3, 3)
+        vals = [float(m[i, j]) for i in range(3) for j in range(3)]
+        flat = vals[0:3] + [0.0] + vals[3:6] + [0.0] + vals[6:9] + [0.0] + [0.0, 0.0, 0.0, 1.0]
+        struct.pack_into("<16f", buf, off, *flat)
+
+
 class Chain(Entity):
     """Chain<A, B>: outer A after inner B (types/src/map.rs:172-235); value: (a, b)."""
     geo = "Eu"
@@ -700,3 +718,53 @@ def eu_gradient_random_value(seed: int, n_objects: int = 8) -> dict:
                            "colors": [tuple(rng.uniform(0.5, 1.5, 3)), tuple(rng.uniform(0.0, 0.3, 3))],
                            "power": float(rng.uniform(0.5, 4.0))},
             "object": objs}
+
+
+def eu_compound_type() -> Struct:
+    """A Euclidean scene type that no example builds, for the containers and maps the examples
+    leave out: one mapped object (map Chain<Linear3, Shift3>) covered with the eu.rs mixture,
+    whose shape is a vector of mapped shapes (maps Chain<Shift3, Linear3>) choosing plane /
+    sphere / cube; gradient background."""
+    shape = ShapeChoice("Eu", ("Plane", PlaneEu()), ("Sphere", Sphere()), ("Cube", Cube()))
+    shapes = ShapeVec("Eu", MappedShape("Eu", shape, Chain(Shift3(), Linear3())))
+    obj = MappedObject("Eu", Covered("Eu", shapes, eu_gradient_material()), Chain(Linear3(), Shift3()))
+    return SceneImpl("Eu", MappedView("Eu", PointView("Eu"), Homogenous3()), obj, GradBg())
+
+
+def _random_linear(rng: np.random.Generator, lo: float = 0.5, hi: float = 1.5, max_angle: float = np.pi) -> np.ndarray:
+    """Rotation (angle <= max_angle) x shear x scale in [lo, hi]."""
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    a = float(rng.uniform(-max_angle, max_angle))
+    k = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    q = np.eye(3) + np.sin(a) * k + (1 - np.cos(a)) * (k @ k)
+    shear = np.eye(3) + np.triu(rng.uniform(-0.3, 0.3, (3, 3)), 1)
+    return q @ shear @ np.diag(rng.uniform(lo, hi, 3))
+
+
+def eu_compound_random_value(seed: int, n_shapes: int = 6) -> dict:
+    """A random scene of eu_compound_type(): a ground plane and spheres / cubes under random
+    linear maps (scale, shear, rotation), one random mixture, a camera in front."""
+    from . import scene as S
+    rng = np.random.default_rng(seed)
+    shapes = [{"map": ((0.0, 0.0, -1.5), np.eye(3)), "inner": ("Plane", None)}]
+    for _ in range(n_shapes - 1):
+        shapes.append({"map": (tuple(rng.uniform(-2.5, 2.5, 2)) + (float(rng.uniform(-0.5, 1.5)),),
+                               _random_linear(rng)),
+                       "inner": (("Sphere", "Cube")[int(rng.integers(2))], None)})
+    p = rng.dirichlet([1.0, 1.0, 1.0])
+    material = {"diffuse": {"material": {"color": tuple(rng.uniform(0.2, 0.9, 3)), "inner": None}, "portion": float(p[0])},
+                "specular": {"material": None, "portion": float(p[1])},
+                "refractive": {"material": {"color": tuple(rng.uniform(0.5, 1.0, 3)),
+                                            "inner": {"index": float(rng.uniform(1.1, 1.8))}},
+                               "portion": float(p[2])}}
+    obj = {"map": (_random_linear(rng, 0.8, 1.2, 0.3), tuple(rng.uniform(-0.3, 0.3, 3))),
+           "inner": {"material": material, "shape": shapes}}
+    q = S.quat_axis_angle([1.0, 0.0, 0.0], float(rng.uniform(-0.2, 0.2)))
+    cam = ((float(rng.uniform(-0.5, 0.5)), float(rng.uniform(-0.5, 0.5)), float(rng.uniform(6, 8))), tuple(q))
+    d = rng.normal(size=3)
+    return {"view": {"map": cam, "inner": {"fov": float(rng.uniform(0.7, 1.3))}},
+            "background": {"direction": tuple(d / np.linalg.norm(d)),
+                           "colors": [tuple(rng.uniform(0.5, 1.5, 3)), tuple(rng.uniform(0.0, 0.3, 3))],
+                           "power": float(rng.uniform(0.5, 4.0))},
+            "object": obj}

@@ -584,7 +584,7 @@ static int render_ext(int recipe, uint32_t hops, const uint8_t *scene, size_t sc
 int HTO(render)(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, int address_width,
                 uint32_t W, uint32_t H, const uint32_t *pixels, size_t n_pixels, uint32_t passes,
                 float *canvas, uint32_t *seeds, uint32_t flags, int threads, uint64_t *stats) {
-    if (recipe == 3 || recipe == 4)
+    if (recipe == 3 || recipe == 4 || recipe == 5)
         return render_ext(recipe, hops, scene, scene_len, address_width, W, H, pixels, n_pixels, passes, canvas,
                           seeds, flags, threads, stats);
     if (hops == 0) return -3;
@@ -682,6 +682,12 @@ typedef struct {
     uint32_t shape;
 } gr_object;
 
+/* Linear3 (transform/linear.cc, algebra/matrix_real.cc): 16 reals, rows padded. */
+typedef struct { R m[16]; } m33;
+/* Recipe 5: one object (map Chain<Linear3, Shift3>) whose shape is a vector of mapped shapes
+ * (maps Chain<Shift3, Linear3>); the material of recipe 4's objects. */
+typedef struct { vec3 shift; m33 lin; vec3 shift_inv; m33 lin_inv; uint32_t shape; } cp_shape;
+
 typedef struct {
     int recipe;
     uint32_t n;
@@ -692,7 +698,64 @@ typedef struct {
     vec3 grad_dir; col3 grad_c0, grad_c1; float grad_power;
     tl_object *tl;
     gr_object *gr;
+    /* recipe 5 */
+    m33 obj_lin, obj_lin_inv;
+    vec3 obj_shift, obj_shift_inv;
+    gr_object cp_mat;
+    cp_shape *cp;
 } ext_scene_t;
+
+static inline vec3 r33_mv(const m33 *a, vec3 b) {   /* r44_dot_mv(a, (b, 0)).xyz */
+    const R *m = a->m;
+    R x = 0; x += m[0] * b.x; x += m[1] * b.y; x += m[2] * b.z; x += m[3] * (R)0;
+    R y = 0; y += m[4] * b.x; y += m[5] * b.y; y += m[6] * b.z; y += m[7] * (R)0;
+    R z = 0; z += m[8] * b.x; z += m[9] * b.y; z += m[10] * b.z; z += m[11] * (R)0;
+    return v3(x, y, z);
+}
+static inline m33 r33_tr(const m33 *a) {
+    m33 t;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) t.m[4 * i + j] = a->m[4 * j + i];
+    return t;
+}
+static inline m33 r33_inv(const m33 *a) {   /* matrix_real.cc:106-120 */
+    const R *m = a->m;
+    R det = m[0] * m[5] * m[10] + m[1] * m[6] * m[8] + m[2] * m[4] * m[9]
+          - m[0] * m[6] * m[9] - m[1] * m[4] * m[10] - m[2] * m[5] * m[8];
+    R adj[16] = {m[5] * m[10] - m[6] * m[9], m[2] * m[9] - m[1] * m[10], m[1] * m[6] - m[2] * m[5], 0,
+                 m[6] * m[8] - m[4] * m[10], m[0] * m[10] - m[2] * m[8], m[2] * m[4] - m[0] * m[6], 0,
+                 m[4] * m[9] - m[5] * m[8], m[1] * m[8] - m[0] * m[9], m[0] * m[5] - m[1] * m[4], 0,
+                 0, 0, 0, 0};
+    m33 r;
+    for (int i = 0; i < 16; ++i) r.m[i] = adj[i] / det;
+    r.m[15] = (R)1;
+    return r;
+}
+static inline vec3 lin_normal(const m33 *l, vec3 d) {   /* lin3_apply_normal */
+    m33 inv = r33_inv(l);
+    m33 it = r33_tr(&inv);
+    return normalize3(r33_mv(&it, d));
+}
+/* Chain<Linear3, Shift3> (outer linear after inner shift, chain.inl:36-73): ray map */
+static inline ray_eu ray_ls(ray_eu r, const m33 *l, vec3 s) {
+    ray_eu o;
+    o.start = r33_mv(l, v3(r.start.x + s.x, r.start.y + s.y, r.start.z + s.z));
+    o.dir = normalize3(normalize3(r33_mv(l, r.dir)));
+    return o;
+}
+/* Chain<Shift3, Linear3> (outer shift after inner linear): ray map */
+static inline ray_eu ray_sl(ray_eu r, vec3 s, const m33 *l) {
+    ray_eu o;
+    vec3 p = r33_mv(l, r.start);
+    o.start = v3(p.x + s.x, p.y + s.y, p.z + s.z);
+    o.dir = normalize3(normalize3(r33_mv(l, r.dir)));
+    return o;
+}
+static m33 rd_lin(const uint8_t *b) {
+    m33 m;
+    for (int i = 0; i < 16; ++i) m.m[i] = rd_f(b, 4 * i);
+    return m;
+}
 
 static col3 rd_col(const uint8_t *b, size_t off) { col3 c = {rd_f(b, off), rd_f(b, off + 4), rd_f(b, off + 8)}; return c; }
 
@@ -740,6 +803,42 @@ static int ext_parse(int recipe, const uint8_t *b, size_t len, int aw, ext_scene
     s->grad_c0 = rd_col(b, 64);
     s->grad_c1 = rd_col(b, 80);
     s->grad_power = rd_f(b, 96);
+    if (recipe == 5) {
+        /* object map Chain<Linear3, Shift3> @128 (linear @128, shift @192); material @256;
+         * shape vector: count @384, elements @448 + 192 i (shift @0, linear @64, choice @128) */
+        if (len < 448) return -1;
+        s->obj_lin = rd_lin(b + 128);
+        s->obj_shift = v3(rd_f(b, 192), rd_f(b, 196), rd_f(b, 200));
+        /* chain inverse: outer^-1, inner^-1, then shf3_lin3_reorder (linear.cc) */
+        s->obj_lin_inv = r33_inv(&s->obj_lin);
+        {
+            m33 back = r33_inv(&s->obj_lin_inv);
+            s->obj_shift_inv = r33_mv(&back, v3(-s->obj_shift.x, -s->obj_shift.y, -s->obj_shift.z));
+        }
+        gr_object *g = &s->cp_mat;
+        g->diffuse_color = rd_col(b, 256);
+        g->diffuse = rd_f(b, 272);
+        g->specular = rd_f(b, 288);
+        g->refr_color = rd_col(b, 304);
+        g->refr_index = rd_f(b, 320);
+        g->refr = rd_f(b, 336);
+        s->n = rd_u(b, 384);
+        if (aw == 64 && rd_u(b, 388) != 0) return -1;
+        if ((len - 448) / 192 < s->n) return -1;
+        s->cp = (cp_shape *)calloc(s->n ? s->n : 1, sizeof(cp_shape));
+        for (uint32_t i = 0; i < s->n; ++i) {
+            const uint8_t *o = b + 448 + (size_t)i * 192;
+            cp_shape *c = &s->cp[i];
+            c->shift = v3(rd_f(o, 0), rd_f(o, 4), rd_f(o, 8));
+            c->lin = rd_lin(o + 64);
+            c->shape = rd_u(o, 128);
+            if ((aw == 64 && rd_u(o, 132) != 0) || c->shape > 2) { free(s->cp); return -5; }
+            /* Chain<Shift3, Linear3> inverse: -shift, lin^-1, then lin3_shf3_reorder */
+            c->lin_inv = r33_inv(&c->lin);
+            c->shift_inv = r33_mv(&c->lin_inv, v3(-c->shift.x, -c->shift.y, -c->shift.z));
+        }
+        return 0;
+    }
     s->n = rd_u(b, 112);
     if (aw == 64 && rd_u(b, 116) != 0) return -1;
     if ((len - 128) / 128 < s->n) return -1;
@@ -1138,6 +1237,74 @@ static col3 sample_gr(const ext_scene_t *sc, uint32_t hops, uint32_t *rng, R px,
     return emission;
 }
 
+/* Recipe 5 hop loop: the object (object/mapped.inl) -> covered (object/covered.inl) ->
+ * shape vector (shape/vector.inl: nearest hit, ties to the lowest index, hash = index) ->
+ * mapped shapes (shape/mapped.inl: local hit, normal through apply_normal, ray mapped back). */
+static col3 sample_cp(const ext_scene_t *sc, uint32_t hops, uint32_t *rng, R px, R py, R size, uint32_t flags,
+                      stats_t *st) {
+    R u0 = rng_uniform(rng);
+    R u1 = rng_uniform(rng);
+    R jx = (flags & HTO_JITTER_YX) ? u1 : u0;
+    R jy = (flags & HTO_JITTER_YX) ? u0 : u1;
+    R sx = px + size * (jx - (R)0.5f);
+    R sy = py + size * (jy - (R)0.5f);
+    vec3 ld = normalize3(v3(sx, sy, (R)-1 / sc->fov));
+    ray_eu ray;
+    ray.dir = hom3_apply_dir(sc->cam_hom, ld);
+    ray.start = hom3_apply_pos(sc->cam_hom, v3((R)0, (R)0, (R)0));
+    col3 intensity = {1.0f, 1.0f, 1.0f};
+    col3 emission = {0.0f, 0.0f, 0.0f};
+    uint32_t prev_hash = 0xFFFFFFFFu;
+    st->samples += 1;
+    for (uint32_t i = 0; i < hops; ++i) {
+        st->hops += 1;
+        st->object_tests += 1;
+        ray_eu local = ray_ls(ray, &sc->obj_lin_inv, sc->obj_shift_inv);
+        R min_dist = (R)-1;
+        uint32_t min_index = 0;
+        ray_eu min_hit = {{0, 0, 0}, {0, 0, 0}};
+        vec3 min_normal = {0, 0, 0};
+        for (uint32_t k = 0; k < sc->n; ++k) {
+            int repeat = (k == prev_hash);
+            const cp_shape *c = &sc->cp[k];
+            ray_eu sl = ray_sl(local, c->shift_inv, &c->lin_inv);
+            vec3 n;
+            R dist = c->shape == 0 ? plane_eu_detect(repeat, &n, &sl)
+                   : c->shape == 1 ? sphere_eu_detect(repeat, &n, &sl)
+                                   : cube_eu_detect(repeat, &n, &sl);
+            if (dist > -EPS && (min_dist <= -EPS || dist < min_dist)) {
+                min_dist = dist; min_index = k; min_hit = sl; min_normal = n;
+            }
+        }
+        if (min_dist > -EPS) {
+            st->hits += 1;
+            const cp_shape *c = &sc->cp[min_index];
+            vec3 normal = lin_normal(&c->lin, min_normal);            /* shf3 normal = identity */
+            ray_eu hit_obj = ray_sl(min_hit, c->shift, &c->lin);       /* shape map back */
+            ray_eu world = ray_ls(hit_obj, &sc->obj_lin, sc->obj_shift);   /* object map back */
+            ray_eu loc = ray_ls(world, &sc->obj_lin_inv, sc->obj_shift_inv);
+            int ret = gr_material_interact(&sc->cp_mat, rng, normal, &loc.dir, &intensity);
+            ray = ray_ls(loc, &sc->obj_lin, sc->obj_shift);
+            if (!ret) break;
+            prev_hash = min_index;
+        } else {
+            /* object/mapped.inl:33-35 maps the ray back even when nothing was hit: the
+             * background sees the round-tripped direction */
+            ray = ray_ls(local, &sc->obj_lin, sc->obj_shift);
+            float f = 0.5f * ((float)dot3(ray.dir, sc->grad_dir) + 1.0f);
+            f = f < 0.0f ? 0.0f : f;
+            f = 1.0f < f ? 1.0f : f;
+            f = powf(f, sc->grad_power);
+            float g = 1.0f - f;
+            emission.x += (f * sc->grad_c0.x + g * sc->grad_c1.x) * intensity.x;
+            emission.y += (f * sc->grad_c0.y + g * sc->grad_c1.y) * intensity.y;
+            emission.z += (f * sc->grad_c0.z + g * sc->grad_c1.z) * intensity.z;
+            break;
+        }
+    }
+    return emission;
+}
+
 typedef struct {
     const ext_scene_t *sc;
     uint32_t hops, W, H, passes, flags;
@@ -1170,7 +1337,8 @@ static void *ext_worker_main(void *arg) {
             for (uint32_t p = 0; p < j->passes; ++p) {
                 uint32_t rng = j->seeds[i];
                 col3 c = j->sc->recipe == 3 ? sample_tl(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st)
-                                            : sample_gr(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st);
+                       : j->sc->recipe == 4 ? sample_gr(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st)
+                                            : sample_cp(j->sc, j->hops, &rng, pxr, pyr, size, j->flags, &w->st);
                 float *cv = j->canvas + 4 * i;
                 cv[0] += c.x; cv[1] += c.y; cv[2] += c.z; cv[3] += 1.0f;
                 j->seeds[i] = rng;
@@ -1209,6 +1377,6 @@ static int render_ext(int recipe, uint32_t hops, const uint8_t *scene, size_t sc
     }
     free(ws); free(ts);
     pthread_mutex_destroy(&job.lock);
-    free(sc.tl); free(sc.gr);
+    free(sc.tl); free(sc.gr); free(sc.cp);
     return 0;
 }

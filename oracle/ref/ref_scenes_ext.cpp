@@ -13,6 +13,11 @@
 //               Vec<Mapped<Covered<Choice{Plane, Sphere, Cube}, Mixture{diffuse: Colored<Lambertian>,
 //                 specular: Specular, refractive: Colored<Refractive>}>, Shift3>>, GradBg, H>
 //                                                                  (main/examples/eu.rs:30-44)
+//   recipe 5  a compound Euclidean type no example builds, for the containers and maps the
+//             examples leave out: SceneImpl<Euclidean3, Mapped<PointView, Homogenous3>,
+//               Mapped<Covered<Vec<Mapped<Choice{Plane, Sphere, Cube}, Chain<Shift3, Linear3>>>,
+//                 Mixture{Colored<Lambertian>, Specular, Colored<Refractive>}>,
+//                 Chain<Linear3, Shift3>>, GradBg, H>
 // Generated struct text and getters follow type-macros/src/source.rs:14-92,171-178,190 and the
 // object choice macros (objects/src/object/choice.rs, kernel/ocl/object/choice/macros.hh);
 // the template instantiation pattern is that of kernel/ocl/render/test/scene_hy.cpp.
@@ -54,6 +59,7 @@
 #include <background/gradient.hh>
 #include <transform/homogenous.hh>
 #include <transform/shift.hh>
+#include <transform/linear.hh>
 #include <shape/choice/macros.hh>
 #include <object/choice/macros.hh>
 #include <material/mixture/macros.hh>
@@ -609,6 +615,205 @@ inline __global const GradBg *gr_scene__background__gc(__global const GrScene *s
 #undef $background
 #undef $light_hops
 
+// ============================================================================ compound type
+// Chain<Shift3, Linear3> and Chain<Linear3, Shift3> (transform/chain.inl)
+#define $Self CpChainSL
+#define $self cp_chain_sl
+#define $Outer Shift3
+#define $outer shf3
+#define $Inner Linear3
+#define $inner lin3
+#define $elem real3
+#include <transform/chain.inl>
+#undef $Self
+#undef $self
+#undef $Outer
+#undef $outer
+#undef $Inner
+#undef $inner
+#undef $elem
+#define $Self CpChainLS
+#define $self cp_chain_ls
+#define $Outer Linear3
+#define $outer lin3
+#define $Inner Shift3
+#define $inner shf3
+#define $elem real3
+#include <transform/chain.inl>
+#undef $Self
+#undef $self
+#undef $Outer
+#undef $outer
+#undef $Inner
+#undef $inner
+#undef $elem
+
+#define $Geo Eu
+#define $geo eu
+#define $Map CpChainSL
+#define $map cp_chain_sl
+#include <geometry/ray_map.inl>
+#undef $Map
+#undef $map
+#define $Map CpChainLS
+#define $map cp_chain_ls
+#include <geometry/ray_map.inl>
+#undef $Map
+#undef $map
+#undef $Geo
+#undef $geo
+
+// Mapped<Choice{Plane, Sphere, Cube}, Chain<Shift3, Linear3>> as a shape (shape/mapped.inl)
+typedef struct CpMShape { CpChainSL map; GrChoice inner; } CpMShape;
+inline __global const ShapeGrChoice *cp_mshape__inner__gc(__global const CpMShape *s) { return &s->inner; }
+#define $Self ShapeCpMShape
+#define $self shape_cp_mshape
+#define $Base CpMShape
+#define $base cp_mshape
+#define $Geo Eu
+#define $geo eu
+#define $Map CpChainSL
+#define $map cp_chain_sl
+#define $Shape ShapeGrChoice
+#define $shape shape_gr_choice
+#include <shape/mapped.inl>
+#undef $Self
+#undef $self
+#undef $Base
+#undef $base
+#undef $Geo
+#undef $geo
+#undef $Map
+#undef $map
+#undef $Shape
+#undef $shape
+
+// Vec<..> as a shape (shape/vector.inl)
+#define $Self CpShapeVector
+#define $self cp_shape_vector
+#define $Element CpMShape
+#define $element_size 192
+#include <container/vector.inl>
+#undef $Self
+#undef $self
+#undef $Element
+#undef $element_size
+#define $Self ShapeCpVector
+#define $self shape_cp_vector
+#define $Base CpShapeVector
+#define $base cp_shape_vector
+#define $Geo Eu
+#define $geo eu
+#define $Shape ShapeCpMShape
+#define $shape shape_cp_mshape
+#include <shape/vector.inl>
+#undef $Self
+#undef $self
+#undef $Base
+#undef $base
+#undef $Geo
+#undef $geo
+#undef $Shape
+#undef $shape
+
+typedef struct CpCovered { GrMixture material; CpShapeVector *shape; } CpCovered;
+typedef struct CpCoveredCache { EuDir normal; } CpCoveredCache;
+inline __global const ShapeCpVector *cp_covered__shape__gc(__global const CpCovered *s) { return s->shape; }
+inline __global const GrMixture *cp_covered__material__gc(__global const CpCovered *s) { return &s->material; }
+#define $Self CpCovered
+#define $self cp_covered
+#define $Geo Eu
+#define $geo eu
+#define $Shape ShapeCpVector
+#define $shape shape_cp_vector
+#define $Material GrMixture
+#define $material gr_mixture
+#define $Cache CpCoveredCache
+#define $cache cp_covered_cache
+#include <object/covered.inl>
+#undef $Self
+#undef $self
+#undef $Geo
+#undef $geo
+#undef $Shape
+#undef $shape
+#undef $Material
+#undef $material
+#undef $Cache
+#undef $cache
+
+typedef struct CpMapped { CpChainLS map; CpCovered inner; } CpMapped;
+inline __global const CpCovered *cp_mapped__inner__gc(__global const CpMapped *s) { return &s->inner; }
+#define $Self ObjectCpMapped
+#define $self object_cp_mapped
+#define $Base CpMapped
+#define $base cp_mapped
+#define $Geo Eu
+#define $geo eu
+#define $Map CpChainLS
+#define $map cp_chain_ls
+#define $Object CpCovered
+#define $object cp_covered
+#define $Cache CpCoveredCache
+#define $cache cp_covered_cache
+#include <object/mapped.inl>
+#undef $Self
+#undef $self
+#undef $Base
+#undef $base
+#undef $Geo
+#undef $geo
+#undef $Map
+#undef $map
+#undef $Object
+#undef $object
+#undef $Cache
+#undef $cache
+
+typedef CpMapped CountedCp;
+static real counted_cp_detect(__global const CountedCp *self, Context *context, CpCoveredCache *cache, LightEu *light) {
+    t_ext.hops += 1;
+    t_ext.object_tests += 1;
+    real d = object_cp_mapped_detect(self, context, cache, light);
+    if (d > (real)-0.5f) t_ext.hits += 1;
+    return d;
+}
+static bool counted_cp_interact(__global const CountedCp *self, Context *context, CpCoveredCache *cache, LightEu *light, color3 *emission) {
+    return object_cp_mapped_interact(self, context, cache, light, emission);
+}
+
+typedef struct CpScene { GrView view; GradBg background; CpMapped object; } CpScene;
+inline __global const ViewGrView *cp_scene__view__gc(__global const CpScene *s) { return &s->view; }
+inline __global const CountedCp *cp_scene__object__gc(__global const CpScene *s) { return &s->object; }
+inline __global const GradBg *cp_scene__background__gc(__global const CpScene *s) { return &s->background; }
+#define $Self CpScene
+#define $self cp_scene
+#define $Geo Eu
+#define $geo eu
+#define $View ViewGrView
+#define $view view_gr_view
+#define $Object CountedCp
+#define $object counted_cp
+#define $ObjectCache CpCoveredCache
+#define $object_cache cp_covered_cache
+#define $Background GradBg
+#define $background grad_bg
+#define $light_hops g_ext_hops
+#include <render/scene.inl>
+#undef $Self
+#undef $self
+#undef $Geo
+#undef $geo
+#undef $View
+#undef $view
+#undef $Object
+#undef $object
+#undef $ObjectCache
+#undef $object_cache
+#undef $Background
+#undef $background
+#undef $light_hops
+
 // ============================================================================ parsing
 namespace {
 
@@ -643,12 +848,20 @@ template <typename T, int N> void rd_tiled(const uint8_t *b, size_t off, T *t, T
     (void)t;
 }
 
-constexpr size_t TL_STRIDE = 384, GR_STRIDE = 128;
+constexpr size_t TL_STRIDE = 384, GR_STRIDE = 128, CP_STRIDE = 192;
+
+// Linear3: 16 floats, rows padded (types/src/primitive/matrix.rs:117-165)
+Linear3 rdlin(const uint8_t *b, size_t off) {
+    Linear3 m;
+    for (int i = 0; i < 16; ++i) m.v.s[i] = (real)rdf(b, off + 4 * i);
+    return m;
+}
 
 struct ExtScene {
     int recipe = 0;
     TlScene tl;
     GrScene gr;
+    CpScene cp;
     std::vector<uint8_t> storage;
 };
 
@@ -718,6 +931,43 @@ int parse_ext(int recipe, const uint8_t *b, size_t len, ExtScene *s) {
         s->gr.object = v;
         return 0;
     }
+    if (recipe == 5) {
+        // view Homogenous3 @0, fov @32, GradBg @48..112, object @128: map Chain<Linear3, Shift3>
+        // (linear @128, shift @192), material @256 (as recipe 4 at +240), shape Vec: count @384,
+        // elements @448 + 192 i: map Chain<Shift3, Linear3> (shift @0, linear @64), choice @128.
+        if (len < 448) return -1;
+        s->cp.view.map.outer.v = rdr3(b, 0);
+        s->cp.view.map.inner.v = quat((real)rdf(b, 16), (real)rdf(b, 20), (real)rdf(b, 24), (real)rdf(b, 28));
+        s->cp.view.inner.fov = (real)rdf(b, 32);
+        s->cp.background.direction = rdr3(b, 48);
+        s->cp.background.colors[0] = rdc(b, 64);
+        s->cp.background.colors[1] = rdc(b, 80);
+        s->cp.background.power = rdf(b, 96);
+        s->cp.object.map.outer = rdlin(b, 128);
+        s->cp.object.map.inner.v = rdr3(b, 192);
+        GrMixture &m = s->cp.object.inner.material;
+        m.diffuse.material.color = rdc(b, 256);
+        m.diffuse.portion = (real)rdf(b, 272);
+        m.specular.portion = (real)rdf(b, 288);
+        m.refractive.material.color = rdc(b, 304);
+        m.refractive.material.inner.index = (real)rdf(b, 320);
+        m.refractive.portion = (real)rdf(b, 336);
+        const uint32_t n = rdu(b, 384);
+        if (len < 448 + (size_t)n * CP_STRIDE) return -1;
+        s->storage.assign(sizeof(CpShapeVector) + (n ? n : 1) * sizeof(CpMShape), 0);
+        CpShapeVector *v = reinterpret_cast<CpShapeVector *>(s->storage.data());
+        v->size = n;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint8_t *o = b + 448 + (size_t)i * CP_STRIDE;
+            CpMShape *e = &v->elements[i];
+            e->map.outer.v = rdr3(o, 0);
+            e->map.inner = rdlin(o, 64);
+            e->inner.index = rdu(o, 128);
+            if (e->inner.index > 2) return -1;
+        }
+        s->cp.object.inner.shape = v;
+        return 0;
+    }
     return -2;
 }
 
@@ -727,7 +977,9 @@ void render_ext_pixel(const ExtScene &s, uint32_t W, uint32_t H, uint32_t px, fl
     real2 size = real2((real)2 / (real)H);
     Context context;
     context.rng.state = *seed;
-    color3 c = s.recipe == 3 ? tl_scene_sample(&s.tl, &context, pos, size) : gr_scene_sample(&s.gr, &context, pos, size);
+    color3 c = s.recipe == 3 ? tl_scene_sample(&s.tl, &context, pos, size)
+             : s.recipe == 4 ? gr_scene_sample(&s.gr, &context, pos, size)
+                             : cp_scene_sample(&s.cp, &context, pos, size);
     t_ext.samples += 1;
     canvas4[0] += c.x;
     canvas4[1] += c.y;
@@ -742,7 +994,7 @@ std::mutex g_ext_mutex;
 
 extern "C" {
 
-// htref_render for recipes 3 and 4 (same arguments and semantics).
+// htref_render for recipes 3, 4 and 5 (same arguments and semantics).
 int htref_render_ext(int recipe, uint32_t hops, const uint8_t *scene, size_t scene_len, uint32_t W, uint32_t H,
                      const uint32_t *pixels, size_t n_pixels, uint32_t passes, float *canvas, uint32_t *seeds,
                      int threads, uint64_t *stats) {

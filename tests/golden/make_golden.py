@@ -74,3 +74,7 @@ if __name__ == "__main__":
                   800, 600, 800, 3, 7)
     bytes_fixture("eu_gradient_800x600", T.serialize(T.eu_gradient_type(), T.eu_example_value()), 4, 4, 0x5EED0006,
                   800, 600, 800, 3, 8)
+    # a type no example builds (Linear3 chains both ways, shape vector of mapped shapes): the
+    # oracle's recipe id 5; the CUDA path compiles it at run time
+    bytes_fixture("eu_compound_640x480", T.serialize(T.eu_compound_type(), T.eu_compound_random_value(3, 7)), 5, 6,
+                  0x5EED0008, 640, 480, 800, 3, 9)

@@ -181,3 +181,31 @@ def test_generic_errors(built):
     # the program stays usable after the error
     cv, sd = _run(r, data, 8, 8, np.ones(64, dtype=np.uint32), 1)
     assert np.all(cv[:, 3] == 1.0)
+
+
+def test_nvrtc_compound_type_matches_reference(built):
+    """A type no example builds, served only by the run-time compiler: one mapped object
+    (Chain<Linear3, Shift3>) whose shape is a vector of mapped shapes (Chain<Shift3, Linear3>),
+    gradient background. Against the reference's fixture (g++ draw order) and the C port on a
+    fresh scene (OpenCL draw order)."""
+    f = np.load(os.path.join(GOLDEN, "eu_compound_640x480.npz"))
+    W, H, passes, pix = int(f["width"]), int(f["height"]), int(f["passes"]), f["pixels"]
+    ctx = P.Context(0)
+    ty = T.eu_compound_type()
+    r = P.Render.build(ctx, ty, int(f["hops"]), _lib.HTC_FLAG_JITTER_YX)
+    assert r.static_size() == T.static_size(ty)
+    seeds = np.zeros(W * H, dtype=np.uint32)
+    seeds[pix] = f["seeds_in"]
+    cv, sd = _run(r, f["scene"].tobytes(), W, H, seeds, passes)
+
+    class Ref:
+        canvas = f["canvas_out"]
+        seeds = f["seeds_out"]
+    _compare(cv[pix], sd[pix], Ref, "golden eu_compound_640x480", min_exact=GRADIENT_MIN_EXACT)
+    val = T.eu_compound_random_value(8, 9)
+    data = T.serialize(ty, val)
+    W, H = 96, 64
+    seeds = S.pixel_seeds(8, W * H)
+    cv, sd = _run(P.Render.build(ctx, ty, 6), data, W, H, seeds, 2)
+    ref = oracle.render(data, 5, 6, W, H, np.arange(W * H), seeds, passes=2, threads=8)
+    _compare(cv, sd, ref, "compound random", min_exact=GRADIENT_MIN_EXACT, max_mismatch=RANDOM_MAX_MISMATCH)

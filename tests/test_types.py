@@ -48,6 +48,28 @@ def test_example_type_layouts(aw):
     assert diff == []
 
 
+@pytest.mark.parametrize("aw", [32, 64])
+def test_compound_type_layout(aw):
+    """Offsets the reference's instantiation and the C port read (oracle/ref/ref_scenes_ext.cpp):
+    object map Chain<Linear3, Shift3> @128 (linear @128, shift @192), material @256, shape
+    vector count @384, elements @448 + 192 i (shift @0, linear @64, choice @128)."""
+    W = aw // 8
+    ty = T.eu_compound_type()
+    assert ty.offsets(W) == [0, 0, 48, 128] and T.static_size(ty, aw) == 448
+    obj = ty.fields[3][1]
+    assert obj.offsets(W) == [0, 0, 128] and obj.fields[1][1].lay(W) == (128, 64)
+    cov = obj.fields[2][1]
+    assert cov.offsets(W) == [0, 0, 128]
+    elem = cov.fields[2][1].elem
+    assert elem.lay(W) == (192, 64) and elem.offsets(W) == [0, 0, 128]
+    val = T.eu_compound_random_value(1, 5)
+    data = T.serialize(ty, val, aw)
+    assert len(data) == 448 + 5 * 192
+    lin = np.frombuffer(data[128:192], dtype=np.float32).reshape(4, 4)
+    assert np.allclose(lin[:3, :3], val["object"]["map"][0], atol=1e-6) and list(lin[3]) == [0, 0, 0, 1]
+    assert list(lin[:3, 3]) == [0, 0, 0]
+
+
 def test_cxx_names():
     assert T.hy_tiled_type().cxx().startswith("SceneImpl<Hy, MappedView<Hy, PointView<Hy>, Moebius>, ObjectVec<Hy,")
     assert "ShapeChoice<Eu, PlaneEu, Sphere, Cube>" in T.eu_gradient_type().cxx()
@@ -57,11 +79,14 @@ def test_cxx_names():
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("seed", [11, 22, 33])
-@pytest.mark.parametrize("recipe", [3, 4])
+@pytest.mark.parametrize("recipe", [3, 4, 5])
 def test_port_matches_reference_example_types(built, seed, recipe):
     if recipe == 3:
         data = T.serialize(T.hy_tiled_type(), T.hy_tiled_random_value(seed, n_objects=6))
         hops = 4
+    elif recipe == 5:   # the compound type: Linear3 chains, shape vector of mapped shapes
+        data = T.serialize(T.eu_compound_type(), T.eu_compound_random_value(seed, 7))
+        hops = 6
     else:
         data = T.serialize(T.eu_gradient_type(), T.eu_gradient_random_value(seed, n_objects=7))
         hops = 5
