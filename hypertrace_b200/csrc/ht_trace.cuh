@@ -228,6 +228,7 @@ HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint
 constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
 
 constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
+constexpr float HORO_M = 1e-3f;      // relative margin of the horosphere root bounds
 
 struct Cull { float S, E, T; };   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
 
@@ -321,32 +322,78 @@ HT_D bool culled(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
         const bool point = Fa > 2.0f * t * c.S;
         return away || far || point;
     } else {
-        // The reference accepts a root up to EPS *behind* the start before dividing by
-        // |d.xy|^2 (shape/hy/horosphere.cc:18-25), which for nearly vertical local
-        // directions means a crossing behind the ray can be reported. So the bounds hold
-        // for every point of the horosphere (point), for every crossing (no_root), for the
-        // entry when it lies ahead (entry_far), or for the nearer of both crossings when
-        // either may be reported (inside_far, away_far).
-        const float Flo = F - eF, Fhi = F + eF;
-        const float Wlo = W - eW, Whi = W + eW;
-        const float aW = fabsf(W) + eW;
-        const bool outside = Flo > 1.01f * t;    // P > 1.01
-        const bool inside = Fhi < 0.99f * t;     // P < 0.99
-        const bool approach = Whi < 0.0f;        // V < 0
-        const bool away = Wlo > 0.001f * t;      // V > 0.001
-        // K^2 = P^2 - V^2 > 1.02: the geodesic never reaches the horosphere
-        const bool no_root = Flo > 0.0f && fmaf(Flo, Flo, -aW * aW) > 1.02f * t * t;
-        // entering ahead: e^s >= (P - V) / 2 beyond the threshold
-        const bool entry_far = outside && approach && (Flo - Whi) > 2.02f * c.E * t;
-        // inside: crossings at e^s = (P - V)/(1 + r) < 1 (behind) and (1 + r)/(P + V); both
-        // farther than the threshold when (P - V) E < 1 and (P + V) E < 1
-        const bool inside_far = inside && (Fhi - Wlo) * c.E < 0.99f * t && (Fhi + Whi) * c.E < 0.99f * t;
-        // outside moving away: both crossings behind, the nearer at e^s = (1 + r)/(P + V) <= 2/(P + V)
-        const bool away_far = outside && away && (Flo + Wlo) > 2.02f * c.E * t;
-        // every point of the horosphere is farther than the threshold
-        const bool point = t > c.E * Fhi || t * c.E < Flo;
-        return no_root || entry_far || inside_far || away_far || point;
+        // In the object's frame the reference's horosphere test (shape/hy/horosphere.cc:4-34)
+        // looks at two roots; with P = F/t (1 / local height), V = W/t (its derivative along
+        // the ray), r^2 = 1 - P^2 + V^2 their parameters are t1 = -(V + rP)/P^2 and
+        // t2 = (rP - V)/P^2, and a root is reported only when its parameter is >= -EPS (it
+        // accepts roots up to EPS behind the start, before dividing by |d.xy|^2). The roots
+        // are the crossings at e^s = (P - V)/(1 + r) and (1 + r)/(P + V). The object is
+        // culled when every root that can be reported lies farther than the threshold.
+        const float Flo = F - eF, Fhi = F + eF, Wlo = W - eW, Whi = W + eW;
+        const float aWlo = fmaxf(fabsf(W) - eW, 0.0f), aWhi = fabsf(W) + eW;
+        if (t > c.E * Fhi || t * c.E < Flo) return true;   // every point farther than the threshold
+        if (!(Flo > 0.0f)) return false;
+        const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
+        if (R2hi < -HORO_M * t * t) return true;        // no crossing
+        if (R2lo < HORO_M * t * t) return false;        // nearly tangent: test exactly
+        const float Rlo = sqrtf(R2lo) * (1.0f - 1e-6f), Rhi = sqrtf(R2hi) * (1.0f + 1e-6f);   // r t
+        // margin of the reference's own root test: 2 EPS plus its float error
+        const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
+        const bool r1 = !(Wlo * t + Rlo * Flo > tol);   // root 1 may be reported
+        const bool r2 = !(Wlo * t - Rhi * Fhi > tol);   // root 2 may be reported
+        const float E1 = c.E * (1.0f + HORO_M);
+        const bool r1_far = (Flo - Whi) > E1 * (t + Rhi) || (Fhi - Wlo) * E1 < (t + Rlo);
+        const bool r2_far = (Flo + Wlo) > 0.0f && ((t + Rlo) > E1 * (Fhi + Whi) || (t + Rhi) * E1 < (Flo + Wlo));
+        return (!r1 || r1_far) && (!r2 || r2_far);
     }
+}
+
+// Upper estimate of the nearest hit among objects [0, n) that the reference surely reports:
+// geodesic planes the ray crosses ahead (tanh of the crossing = |F| / |W|) and horospheres
+// entered ahead from outside or left ahead from inside (e^s of the crossing), with margins
+// far above the float error of either side. +inf when none qualifies. A threshold derived from
+// it (cull_from_dist) then culls before the first exact test.
+HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, uint32_t prev_hash) {
+    float best_tanh = 2.0f, best_exp = __int_as_float(0x7f800000);
+    const float t = r.t;
+    for (uint32_t k = 0; k < n; ++k) {   // warp-uniform: broadcast loads
+        const float4 rec = s.bound[k];
+        const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
+        const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+        const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
+        const float W = fmaf(t, G, -F * r.vz);
+        const float eW = fmaf(BOUND_EPS * t, fmaf(2.0f * fabsf(rec.x), fabsf(r.pv), fmaf(fabsf(rec.y), fabsf(r.vx), fabsf(rec.z * r.vy))),
+                              eF * fabsf(r.vz) + BOUND_EPS * fabsf(W));
+        if (s.shape[k] == 0) {
+            if (k == prev_hash) continue;   // a plane is never hit twice in a row
+            const float Fa = fabsf(F) - eF, Wlo = fabsf(W) - eW;
+            if (!((F > 0.0f) != (W > 0.0f) && Fa > 0.02f * t && Wlo > 0.0f)) continue;
+            const float rr = (fabsf(F) + eF) / Wlo;
+            if (rr < 0.99f) best_tanh = fminf(best_tanh, rr);
+        } else {
+            const float Flo = F - eF, Fhi = F + eF, Wlo = W - eW, Whi = W + eW;
+            if (Fhi < 0.999f * t && Flo > 0.0f && (Flo + Wlo) > 0.0f) {   // inside: exit ahead
+                const float aWlo = fmaxf(fabsf(W) - eW, 0.0f), aWhi = fabsf(W) + eW;
+                const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
+                if (R2lo > 1e-3f * t * t) {
+                    const float Rlo = sqrtf(R2lo) * (1.0f - 1e-6f), Rhi = sqrtf(R2hi) * (1.0f + 1e-6f);
+                    const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
+                    const bool r1 = !(Wlo * t + Rlo * Flo > tol);
+                    const bool r2_sure = (Wlo * t - Rhi * Fhi) < -tol - 1e-3f * t * t;
+                    if (!r1 && r2_sure) best_exp = fminf(best_exp, (t + Rhi) / (Flo + Wlo) * 1.001f);
+                }
+            } else if (Flo > 1.01f * t && Whi < -0.01f * t) {   // outside, approaching: entry ahead
+                const float aVlo = -Whi / t;
+                const float P = Fhi / t;
+                const float D = 1.0f - P * P + aVlo * aVlo;
+                if (D > 0.02f) best_exp = fminf(best_exp, (Fhi - Wlo) / t / (1.0f + sqrtf(D)));
+            }
+        }
+    }
+    float u = __int_as_float(0x7f800000);
+    if (best_tanh < 1.0f) u = atanhf(best_tanh);
+    if (best_exp < __int_as_float(0x7f800000)) u = fminf(u, logf(best_exp));
+    return u;
 }
 
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
@@ -361,6 +408,10 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const bool can_cull = cull_point_ok(p);
     const BoundRay br = bound_ray(p, v);
     Cull cull = cull_none();
+    if (can_cull) {   // a threshold before the first exact test, from the first chunk's crossings
+        const float u = upper_estimate(s, min(32u, s.n), br, prev_hash);
+        if (u < __int_as_float(0x7f800000)) cull = cull_from_dist(u);
+    }
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
         const uint32_t cn = min(32u, s.n - c0);
         uint32_t mask = 0;
