@@ -32,14 +32,15 @@ using namespace ht;
 thread_local std::string g_last_error;
 
 // Minimum resident blocks per SM requested from ptxas for the render kernels (register cap).
-// Six 128-thread blocks per SM (80 registers) measured fastest for both kernels: the scan
-// is latency-bound on dependent FP32 chains, so resident warps matter more than the few
-// spilled values of the cold per-path state.
+// The scan is latency-bound on dependent FP32 chains, so resident warps matter more than the
+// few spilled values of the cold per-path state. Measured at 1080p / 200 objects: the plain
+// kernel 7 blocks (72 registers) 239.5 Msamples/s against 6: 232, 8: 231, 5: 229; the
+// persistent and batched kernels 6.
 #ifndef HT_PERSIST_MINB
 #define HT_PERSIST_MINB 6
 #endif
 #ifndef HT_PLAIN_MINB
-#define HT_PLAIN_MINB 6
+#define HT_PLAIN_MINB 7
 #endif
 // htc_render_passes: 1 = the persistent kernel, 0 = one launch of the one-pass kernel per pass.
 #ifndef HT_PASSES_PERSISTENT
