@@ -3,9 +3,11 @@
 
 Workload (one GPU): the 1920x1080 hyperbolic scene of 200 objects (60 % horospheres,
 40 % geodesic planes) placed by random det-1 Moebius maps with translation distance up to 6,
-H = 8 light hops, synthetic and seeded (hypertrace_b200.scene.config2). A step is one
-launch of the persistent kernel rendering `--passes` passes over the whole frame (each pass
-is one sample per pixel); the frame's 256 spp are 256 / passes such steps.
+H = 8 light hops, synthetic and seeded (hypertrace_b200.scene.config2). A step renders
+`--passes` passes over the whole frame (each pass is one sample per pixel) through
+htc_render_passes, which runs each pass as wavefronts: one launch of render_wave per hop
+depth over queues of ray states. The frame's 256 spp are 256 / passes such steps. The
+one-pass kernel (one launch per pass) and the persistent kernel are timed beside it.
 
     python bench.py [--gpus N --steps K --warmup W --passes P]
     python bench.py --impl reference      # the reference's own kernel code on the host CPU
@@ -283,8 +285,8 @@ def main():
     all_samples, max_s, all_hops = replicas.aggregate(samples, dev_s, hops, device=dev)
     value = all_samples / max_s / 1e6
 
-    # roofline of render_plain (one launch per pass, `passes` launches per step)
-    launches = args.steps * args.passes
+    # roofline of render_wave (one launch per hop depth, `passes * hops` launches per step)
+    launches = args.steps * args.passes * sc.hops
     exec_flops = (exact * FLOPS_PER_EXACT_TEST + tests * FLOPS_PER_BOUND_TEST + hits * FLOPS_PER_HIT_HOP
                   + samples * FLOPS_PER_SAMPLE + hops * min(ESTIMATE_OBJECTS, sc.n_objects) * FLOPS_PER_ESTIMATE)
     ref_flops = tests * REF_FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
@@ -309,6 +311,25 @@ def main():
         ps = stats.cpu().numpy()
         persistent = {"value": float(ps[0]) / ms / 1e3, "unit": UNIT, "ms_per_launch": ms,
                       "ray_bounces_per_s": float(ps[1]) / ms * 1e3, "kernel": "render_persistent"}
+
+    # ---------------- the one-pass kernel (one launch per pass, the reference's kernel shape)
+    plain = None
+    if rank == 0:
+        stats.zero_()
+        w_ms = []
+        for _ in range(args.steps):
+            l2_flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.passes):
+                render.render(buf, canvas, stats=stats, sync=False)
+            e1.record(stream)
+            w_ms.append((e0, e1))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in w_ms)
+        ws = stats.cpu().numpy()
+        plain = {"value": float(ws[0]) / ms / 1e3, "unit": UNIT, "ms_per_step": ms / args.steps,
+                 "ray_bounces_per_s": float(ws[1]) / ms * 1e3, "kernel": "render_plain, one launch per pass"}
 
     # ---------------- e2e through the public API with host buffers
     e2e = None
@@ -353,7 +374,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": max_s / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wl.name, "width": W, "height": H, "objects": sc.n_objects, "hops": sc.hops,
-                       "passes_per_step": args.passes, "kernel": "render_plain, one launch per pass",
+                       "passes_per_step": args.passes, "kernel": "render_wave, one launch per hop depth",
                        "parallelism": f"replicas{world}",
                        "l2": "flushed between steps (256 MB device write outside the timed events)"},
             "ray_bounces_per_s": all_hops / max_s,
@@ -365,6 +386,7 @@ def main():
                          "flops_per_launch": exec_flops / launches,
                          "reference_count_tflops": ref_flops / launches / per_launch_s / 1e12},
             "persistent": persistent,
+            "plain_one_pass": plain,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clk,

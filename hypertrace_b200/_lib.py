@@ -54,6 +54,7 @@ SIGNATURES = [
     ("htc_render", _i, [_vp, _u32, _u32, _vp, _sz, _vp, _vp, _vp]),
     ("htc_render_ex", _i, [_vp, _u32, _u32, _vp, _sz, _vp, _vp, _vp, _vp]),
     ("htc_render_passes", _i, [_vp, _u32, _u32, _vp, _sz, _vp, _vp, _u32, _vp, _vp]),
+    ("htc_render_wavefront", _i, [_vp, _u32, _u32, _vp, _sz, _vp, _vp, _u32, _vp, _vp]),
     ("htc_render_passes_noalloc", _i, [_i, _u32, _i, _u32, _u32, _u32, _vp, _sz, _vp, _vp, _u32, _vp, _vp, _vp]),
     ("htc_extract", _i, [_u32, _u32, _u32, _vp, _vp, _vp]),
     ("htc_gamma", _i, [_u32, _u32, _f, _vp, _vp, _vp]),

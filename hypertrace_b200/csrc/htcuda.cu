@@ -42,9 +42,12 @@ thread_local std::string g_last_error;
 #ifndef HT_PLAIN_MINB
 #define HT_PLAIN_MINB 7
 #endif
-// htc_render_passes: 1 = the persistent kernel, 0 = one launch of the one-pass kernel per pass.
-#ifndef HT_PASSES_PERSISTENT
-#define HT_PASSES_PERSISTENT 0
+// htc_render_passes: 2 = wavefronts (one launch per hop depth), 1 = the persistent kernel,
+// 0 = one launch of the one-pass kernel per pass. All three give the same bits. Measured at
+// 1920x1080 / 200 objects / H = 8 (Msamples/s): wavefronts 286.9, one-pass kernel 239.3,
+// persistent kernel 208.6.
+#ifndef HT_PASSES_MODE
+#define HT_PASSES_MODE 2
 #endif
 
 // Device error word bits.
@@ -61,6 +64,9 @@ struct htc_program {
     int num_sms;
     int max_smem;
     GenericProgram *generic;   // scene types served by render_generic (htgeneric.cu), else NULL
+    void *wave_buf;            // two wavefront queues (WAVE_SLOT_BYTES per slot each), grown on demand
+    size_t wave_slots;         // slots per queue
+    uint32_t *d_wave_ctr;      // 2 counters per hop depth
 };
 
 // ============================================================================ staging
@@ -335,6 +341,125 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     rewind_queue(queue);
 }
 
+// ============================================================================ wavefront
+// One launch per hop depth. Launch h takes the paths that are still going after h hops
+// from a queue, runs one hop on each and appends the survivors to the other queue; paths
+// that end add their sample to the canvas right there. Hop 0 starts from the pixels
+// (camera ray, no queue read). Warps take 32 queue slots at a time from a counter and
+// append survivors with one atomic per warp, order kept within the warp, so a warp's
+// lanes stay paths that started at neighbouring pixels and ran the same number of hops:
+// no lane idles on a finished path while its warp scans, which is where the one-pass
+// kernel loses a third of its lanes. The hop itself is `hop<R>` unchanged, so the result
+// is bit-identical to render_plain.
+struct WaveQueue {      // ray state, structure of arrays (one float4 load / store each)
+    float4 *p;          // ray start
+    float4 *v;          // ray direction
+    float4 *t;          // intensity xyz, RNG state (bits) in w
+    float4 *e;          // emission xyz, pixel index (bits) in w
+    uint32_t *h;        // previous hit hash
+};
+constexpr size_t WAVE_SLOT_BYTES = 4 * sizeof(float4) + sizeof(uint32_t);
+
+template <int R> __device__ __forceinline__ void path_store(float4 *p, float4 *v, const typename PathOf<R>::T &r) {
+    if constexpr (R == RECIPE_HY) {
+        *p = make_float4(r.p.x, r.p.y, r.p.z, r.p.w);
+        *v = make_float4(r.v.x, r.v.y, r.v.z, r.v.w);
+    } else {
+        *p = make_float4(r.p.x, r.p.y, r.p.z, 0.0f);
+        *v = make_float4(r.v.x, r.v.y, r.v.z, 0.0f);
+    }
+}
+template <int R> __device__ __forceinline__ typename PathOf<R>::T path_load(float4 p, float4 v) {
+    typename PathOf<R>::T r;
+    if constexpr (R == RECIPE_HY) {
+        r.p = q4(p.x, p.y, p.z, p.w);
+        r.v = q4(v.x, v.y, v.z, v.w);
+    } else {
+        r.p = v3(p.x, p.y, p.z);
+        r.v = v3(v.x, v.y, v.z);
+    }
+    return r;
+}
+
+// ctr[0]: slots taken by warps of this launch; ctr[1]: paths appended to `out`.
+// in_count: paths in `in` (NULL for hop 0, which covers the W*H pixels).
+template <int R>
+__global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
+    const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
+    uint32_t W, uint32_t H, uint32_t hops, uint32_t hop_index, uint32_t flags, float4 *__restrict__ canvas,
+    uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err, WaveQueue in, const uint32_t *in_count,
+    WaveQueue out, uint32_t *ctr) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t s_hdr[2];
+    const uint32_t n = in_count ? *reinterpret_cast<const volatile uint32_t *>(in_count) : W * H;
+    if (n == 0 || blockIdx.x * 128u >= n) return;   // nothing for this block: skip the staging
+    float4 *s_inv = smem;
+    float4 *s_bound = smem + 2 * max_objects;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
+    StagedScene s;
+    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr)) return;
+
+    const uint32_t lane = threadIdx.x & 31;
+    const bool last = hop_index + 1 >= hops;
+    uint32_t n_samples = 0, n_hops = 0, n_hits = 0, n_exact = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&ctr[0], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        bool cont = false;
+        typename PathOf<R>::T ray;
+        uint32_t rng = 0, prev_hash = HASH_NEVER, pixel = 0;
+        Col intensity = {1.0f, 1.0f, 1.0f};
+        Col emission = {0.0f, 0.0f, 0.0f};
+        if (i < n) {
+            if (!in_count) {
+                pixel = i;
+                float px, py, size;
+                pixel_pos(i % W, i / W, W, H, px, py, size);
+                rng = seeds[i];
+                ray = camera<R>(s, px, py, size, rng, flags);
+            } else {
+                ray = path_load<R>(in.p[i], in.v[i]);
+                const float4 t = in.t[i], e = in.e[i];
+                intensity.x = t.x; intensity.y = t.y; intensity.z = t.z;
+                rng = __float_as_uint(t.w);
+                emission.x = e.x; emission.y = e.y; emission.z = e.z;
+                pixel = __float_as_uint(e.w);
+                prev_hash = in.h[i];
+            }
+            bool hit;
+            n_hops += 1;
+            const bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
+            n_hits += hit ? 1 : 0;
+            cont = go && !last;
+            if (!cont) {   // the path ends: this pass's sample of the pixel (render.cl:20-26)
+                n_samples += 1;
+                float4 c = canvas[pixel];
+                c.x += emission.x; c.y += emission.y; c.z += emission.z; c.w += 1.0f;
+                canvas[pixel] = c;
+                seeds[pixel] = rng;
+            }
+        }
+        const uint32_t want = __ballot_sync(0xffffffffu, cont);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            uint32_t obase = 0;
+            if (lane == (uint32_t)leader) obase = atomicAdd(&ctr[1], (uint32_t)__popc(want));
+            obase = __shfl_sync(0xffffffffu, obase, leader);
+            if (cont) {
+                const uint32_t j = obase + __popc(want & ((1u << lane) - 1u));
+                path_store<R>(&out.p[j], &out.v[j], ray);
+                out.t[j] = make_float4(intensity.x, intensity.y, intensity.z, __uint_as_float(rng));
+                out.e[j] = make_float4(emission.x, emission.y, emission.z, __uint_as_float(pixel));
+                out.h[j] = prev_hash;
+            }
+        }
+    }
+    flush_stats(stats, n_samples, n_hops, n_hits, n_exact, s.n);
+}
+
 // ============================================================================ batch
 // Many views (scenes, resolutions, pass counts, either recipe) in one persistent launch.
 // Blocks take tiles (view, pixel range) from a global queue; a block stages a view's scene
@@ -504,6 +629,7 @@ template <int R>
 static int set_smem_attr(size_t smem) {
     HTC_CUDA(cudaFuncSetAttribute(render_plain<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HTC_CUDA(cudaFuncSetAttribute(render_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HTC_CUDA(cudaFuncSetAttribute(render_wave<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return HTC_OK;
 }
 
@@ -613,6 +739,8 @@ void htc_program_destroy(htc_program *p) {
     if (!p) return;
     cudaFree(p->d_err);
     if (p->d_queue) cudaFree(p->d_queue);
+    if (p->wave_buf) cudaFree(p->wave_buf);
+    if (p->d_wave_ctr) cudaFree(p->d_wave_ctr);
     if (p->generic) generic_program_destroy(p->generic);
     delete p;
 }
@@ -721,6 +849,83 @@ int htc_render(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t
     return htc_render_ex(p, W, H, scene, scene_size, canvas, seeds, nullptr, stream);
 }
 
+}  // extern "C"
+
+// Queues of W*H slots each (a hop never has more paths than pixels) and the hop counters;
+// allocated on the first call that needs more and kept with the program.
+static int wave_reserve(htc_program *p, size_t slots) {
+    if (!p->d_wave_ctr) {
+        // hop counts are 32-bit; 2 words per hop depth
+        HTC_CUDA(cudaMalloc(&p->d_wave_ctr, 2 * sizeof(uint32_t) * (size_t)p->hops));
+    }
+    slots = (slots + 63) & ~(size_t)63;   // keeps the second queue and every array 16-byte aligned
+    if (p->wave_slots >= slots) return HTC_OK;
+    if (p->wave_buf) {
+        HTC_CUDA(cudaFree(p->wave_buf));
+        p->wave_buf = nullptr;
+        p->wave_slots = 0;
+    }
+    HTC_CUDA(cudaMalloc(&p->wave_buf, 2 * WAVE_SLOT_BYTES * slots));
+    p->wave_slots = slots;
+    return HTC_OK;
+}
+static WaveQueue wave_queue(htc_program *p, int which) {
+    const size_t n = p->wave_slots;
+    uint8_t *b = reinterpret_cast<uint8_t *>(p->wave_buf) + (size_t)which * WAVE_SLOT_BYTES * n;
+    WaveQueue q;
+    q.p = reinterpret_cast<float4 *>(b);
+    q.v = q.p + n;
+    q.t = q.v + n;
+    q.e = q.t + n;
+    q.h = reinterpret_cast<uint32_t *>(q.e + n);
+    return q;
+}
+template <int R>
+static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc, size_t scene_size,
+                       uint32_t max_objects, size_t smem, float4 *cv, uint32_t *seeds, uint32_t passes,
+                       uint64_t *stats, cudaStream_t st) {
+    int per_sm = 0;
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_wave<R>, 128, smem));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)p->num_sms;
+    const uint64_t needed = ((uint64_t)W * H + 127) / 128;
+    if (blocks > needed) blocks = needed;
+    const WaveQueue q[2] = {wave_queue(p, 0), wave_queue(p, 1)};
+    const WaveQueue none = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        HTC_CUDA(cudaMemsetAsync(p->d_wave_ctr, 0, 2 * sizeof(uint32_t) * (size_t)p->hops, st));
+        for (uint32_t h = 0; h < p->hops; ++h) {
+            const WaveQueue in = h == 0 ? none : q[(h - 1) & 1];
+            const uint32_t *in_count = h == 0 ? nullptr : p->d_wave_ctr + 2 * (h - 1) + 1;
+            render_wave<R><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+                                                               p->hops, h, p->flags, cv, seeds, stats, p->d_err, in,
+                                                               in_count, q[h & 1], p->d_wave_ctr + 2 * h);
+        }
+        HTC_CUDA(cudaGetLastError());
+    }
+    return HTC_OK;
+}
+
+extern "C" {
+
+int htc_render_wavefront(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                         float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+    if (p && p->generic) return fail(HTC_ERR_UNSUPPORTED, "the wavefront form serves the built-in recipes only");
+    uint32_t max_objects = 0;
+    size_t smem = 0;
+    int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
+    if (rc) return rc;
+    if (passes == 0) return HTC_OK;
+    rc = wave_reserve(p, (size_t)W * H);
+    if (rc) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint8_t *sc = reinterpret_cast<const uint8_t *>(scene);
+    float4 *cv = reinterpret_cast<float4 *>(canvas);
+    if (p->recipe == HTC_RECIPE_HY)
+        return launch_wave<RECIPE_HY>(p, W, H, sc, scene_size, max_objects, smem, cv, seeds, passes, stats, st);
+    return launch_wave<RECIPE_EU>(p, W, H, sc, scene_size, max_objects, smem, cv, seeds, passes, stats, st);
+}
+
 int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
                       float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
     if (p && p->generic) return render_generic_program(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
@@ -729,11 +934,8 @@ int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene,
     int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
     if (rc) return rc;
     if (passes == 0) return HTC_OK;
-    if (!HT_PASSES_PERSISTENT) {
-        // One launch of the one-pass kernel per pass: measured faster than the persistent
-        // kernel since the culled scan became cheap (1920x1080 / 200 objects / H = 8:
-        // 232 vs 213 Msamples/s; 800x600 / 18 objects: 661 vs 471); the results are the same
-        // bits either way.
+    if (HT_PASSES_MODE == 2) return htc_render_wavefront(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
+    if (HT_PASSES_MODE == 0) {
         for (uint32_t k = 0; k < passes; ++k) {
             int rc2 = htc_render_ex(p, W, H, scene, scene_size, canvas, seeds, stats, stream);
             if (rc2) return rc2;

@@ -157,8 +157,19 @@ class Render:
 
     def render_passes(self, scene_buffer: EntityBuffer, canvas: Canvas, passes: int,
                       stats: Optional[torch.Tensor] = None, sync: bool = True) -> None:
-        """`passes` passes in one persistent launch (bit-identical to `passes` render calls)."""
+        """`passes` passes, each as wavefronts of one launch per hop depth (bit-identical to
+        `passes` render calls)."""
         _lib.call("htc_render_passes", self.handle, canvas.width, canvas.height, scene_buffer.ptr(),
+                  scene_buffer.size, canvas.image.data_ptr(), canvas.seeds.data_ptr(), passes,
+                  None if stats is None else stats.data_ptr(), self.context.stream())
+        self._check(sync)
+        canvas.add_pass(passes)
+
+    def render_wavefront(self, scene_buffer: EntityBuffer, canvas: Canvas, passes: int,
+                         stats: Optional[torch.Tensor] = None, sync: bool = True) -> None:
+        """`passes` passes as wavefronts, one launch per hop depth over queues of ray states
+        (bit-identical to `passes` render calls)."""
+        _lib.call("htc_render_wavefront", self.handle, canvas.width, canvas.height, scene_buffer.ptr(),
                   scene_buffer.size, canvas.image.data_ptr(), canvas.seeds.data_ptr(), passes,
                   None if stats is None else stats.data_ptr(), self.context.stream())
         self._check(sync)

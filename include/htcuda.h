@@ -120,13 +120,23 @@ int htc_stream_sync(void *stream);
 int htc_render(htc_program *program, uint32_t width, uint32_t height, const void *scene,
                size_t scene_size, float *canvas, uint32_t *seeds, void *stream);
 
-/* `passes` successive passes in one persistent launch. The result is bit-identical to
- * `passes` htc_render calls: each pixel's samples run in order on one thread, which keeps
- * its RNG stream, and finished paths are regenerated in place so lanes stay busy.
- * stats (optional, device uint64[HTC_STAT_COUNT]) accumulates the HTC_STAT_* counters. */
+/* `passes` successive passes; bit-identical to `passes` htc_render calls (each pixel's
+ * samples run in order and keep its RNG stream). For the built-in recipes this is
+ * htc_render_wavefront, so the program keeps the queues that form allocates. stats (optional, device uint64[HTC_STAT_COUNT])
+ * accumulates the HTC_STAT_* counters. */
 int htc_render_passes(htc_program *program, uint32_t width, uint32_t height, const void *scene,
                       size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
                       uint64_t *stats, void *stream);
+
+/* `passes` successive passes as wavefronts: per pass, one launch per hop depth runs one hop
+ * of every path still going, from a queue of ray states, and appends the survivors to the
+ * next queue (warp-aggregated, order kept within a warp). Bit-identical to htc_render_passes.
+ * The program keeps two queues of width*height slots (68 bytes each), allocated by the first
+ * call that needs them. No counterpart in the reference (its Render enqueues one kernel per
+ * pass, processing/src/render.rs:102-118). stats as in htc_render_passes. */
+int htc_render_wavefront(htc_program *program, uint32_t width, uint32_t height, const void *scene,
+                         size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
+                         uint64_t *stats, void *stream);
 
 /* Allocation-free form of htc_render_passes, for callers that cannot call cudaMalloc --
  * e.g. hosts that hand the renderer a fixed memory budget, or custom allocators that own

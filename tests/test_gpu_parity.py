@@ -79,6 +79,51 @@ def test_persistent_equals_repeated_plain(built, cfg):
     assert np.array_equal(cv_a.view(np.uint32), cv_b.view(np.uint32))
 
 
+@pytest.mark.parametrize("cfg,W,H,passes", [("config0", 160, 120, 5), ("config1", 200, 150, 3),
+                                           ("config2", 480, 270, 2), ("config1", 33, 7, 4)])
+def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes):
+    """Hop-depth wavefronts over ray-state queues == P plain launches, bit for bit, with the
+    same statistics (samples, hops, hits, exact tests)."""
+    wl = getattr(S, cfg)()
+    ctx = P.Context(0)
+    buf = P.EntityBuffer(ctx, wl.scene)
+    r = P.Render(ctx, wl.scene.recipe, wl.scene.hops)
+    out = []
+    for wave in (False, True):
+        canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
+        stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+        if wave:
+            r.render_wavefront(buf, canvas, passes, stats=stats)
+        else:
+            for _ in range(passes):
+                r.render(buf, canvas, stats=stats)
+        torch.cuda.synchronize()
+        out.append((canvas.image.cpu().numpy().view(np.uint32).copy(), canvas.seeds.cpu().numpy().copy(),
+                    stats.cpu().numpy().copy()))
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert out[1][2][_lib.STAT_SAMPLES] == W * H * passes
+
+
+def test_wavefront_single_hop_and_reuse(built):
+    """H = 1 (hop 0 only, nothing queued) and a program reused across canvas sizes (queues grow)."""
+    wl = S.config1()
+    ctx = P.Context(0)
+    buf = P.EntityBuffer(ctx, wl.scene)
+    for hops in (1, wl.scene.hops):
+        r = P.Render(ctx, wl.scene.recipe, hops)
+        for W, H in ((64, 48), (300, 200), (64, 48)):
+            a = P.Canvas(ctx, (W, H), global_seed=5)
+            b = P.Canvas(ctx, (W, H), global_seed=5)
+            for _ in range(2):
+                r.render(buf, a)
+            r.render_wavefront(buf, b, 2)
+            torch.cuda.synchronize()
+            assert torch.equal(a.seeds, b.seeds)
+            assert torch.equal(a.image.view(torch.int32), b.image.view(torch.int32))
+
+
 @pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("cfg", ["config0", "config1"])
 def test_render_matches_reference_kernel(built, cfg):
