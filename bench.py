@@ -413,10 +413,11 @@ def _time_ms(fn, stream):
 def bench_batched(args):
     """The mixed workload (96 views: resolutions from {256^2, 640x480, 1280x720, 1920x1080},
     spp in {16..256} x --spp-scale, half Euclidean / half hyperbolic with 20-200 objects):
-    batched persistent launches (autotuned tile size / residency, CUDA graphs, 16 passes of
-    every unfinished view per step) against the same views rendered one at a time with the
-    plain one-pass kernel and with the single-view persistent kernel. Results of the three
-    are bit-identical (tests/test_gpu_batch.py), so RMSE against any reference is equal."""
+    batched wavefronts (one launch per pass and hop depth covering every view, autotuned tile
+    size / residency, CUDA graphs, 16 passes of every unfinished view per step) against the
+    same views rendered one at a time with the plain one-pass kernel and with the single-view
+    wavefront form (htc_render_passes). Results of the three are bit-identical
+    (tests/test_gpu_batch.py), so RMSE against any reference is equal."""
     import torch
     from hypertrace_b200 import batch as B
     from hypertrace_b200 import processing as P
@@ -450,7 +451,7 @@ def bench_batched(args):
     for v in views:
         v.release()
 
-    def per_view(persistent):
+    def per_view(wavefront):
         vs = B.config3(spp_scale=args.spp_scale)
         ms = 0.0
         renders = {}
@@ -458,7 +459,7 @@ def bench_batched(args):
             v.allocate(ctx)
             key = (v.scene.recipe, v.scene.hops)
             r = renders.setdefault(key, P.Render(ctx, *key))
-            if persistent:
+            if wavefront:
                 ms += _time_ms(lambda: r.render_passes(v.buffer, v.canvas, v.spp, sync=False), stream)
             else:
                 ms += _time_ms(lambda: [r.render(v.buffer, v.canvas, sync=False) for _ in range(v.spp)], stream)
@@ -467,11 +468,12 @@ def bench_batched(args):
 
     plain = per_view(False)
     single = per_view(True)
-    line = {"metric": "Msamples/s, mixed batched workload (96 views, 1 launch per step)", "value": batched["value"],
+    line = {"metric": "Msamples/s, mixed batched workload (96 views, one launch per pass and hop depth)",
+            "value": batched["value"],
             "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "mixed-96-views", "spp_scale": args.spp_scale, "total_samples": total_samples,
                        "passes_per_step": 16},
-            "batched": batched, "plain_per_view": plain, "persistent_per_view": single,
+            "batched": batched, "plain_per_view": plain, "wavefront_per_view": single,
             "speedup_vs_plain": batched["value"] / plain["value"]}
     print(json.dumps(line), flush=True)
 

@@ -48,7 +48,8 @@ class View:
         return self.spp - self.done_passes
 
     def device_bytes(self) -> int:
-        return self.width * self.height * (16 + 4) + S.scene_size(self.scene.recipe, self.scene.n_objects)
+        # canvas (16 B) and seed (4 B) per pixel, two wavefront queue slots (2 x 68 B) per pixel
+        return self.width * self.height * (16 + 4 + 136) + S.scene_size(self.scene.recipe, self.scene.n_objects)
 
     def descriptor(self, passes: int, address_width: int = 32) -> _lib.HtcView:
         return _lib.HtcView(self.buffer.ptr(), self.buffer.size, self.canvas.image.data_ptr(),

@@ -49,6 +49,10 @@ thread_local std::string g_last_error;
 #ifndef HT_PASSES_MODE
 #define HT_PASSES_MODE 2
 #endif
+// htc_batch_render: 2 = wavefronts (render_batch_wave), 1 = one persistent launch (render_batch).
+#ifndef HT_BATCH_MODE
+#define HT_BATCH_MODE 2
+#endif
 
 // Device error word bits.
 constexpr uint32_t ERR_SCENE = 1u;
@@ -232,7 +236,27 @@ constexpr uint32_t NO_PIXEL = 0xFFFFFFFFu;
 // Counters of one thread, flushed once per launch.
 struct LaneStats {
     uint32_t samples = 0, hops = 0, hits = 0, exact = 0;
+    uint64_t tests = 0;   // object tests the reference makes (hops x objects)
 };
+
+__device__ __forceinline__ void flush_lane_stats(uint64_t *stats, const LaneStats &st) {
+    if (!stats) return;
+    uint64_t samples = st.samples, hops = st.hops, hits = st.hits, exact = st.exact, tests = st.tests;
+    for (int off = 16; off > 0; off >>= 1) {
+        samples += __shfl_down_sync(0xffffffffu, samples, off);
+        hops += __shfl_down_sync(0xffffffffu, hops, off);
+        hits += __shfl_down_sync(0xffffffffu, hits, off);
+        exact += __shfl_down_sync(0xffffffffu, exact, off);
+        tests += __shfl_down_sync(0xffffffffu, tests, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_SAMPLES], (unsigned long long)samples);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_HOPS], (unsigned long long)hops);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_OBJECT_TESTS], (unsigned long long)tests);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_HITS], (unsigned long long)hits);
+        atomicAdd((unsigned long long *)&stats[HTC_STAT_EXACT_TESTS], (unsigned long long)exact);
+    }
+}
 
 // The persistent lane loop shared by render_persistent and render_batch: warps take pixel
 // indices [first, first + count) from `*counter` (global or shared memory) with one atomic
@@ -381,6 +405,79 @@ template <int R> __device__ __forceinline__ typename PathOf<R>::T path_load(floa
     return r;
 }
 
+__host__ __device__ inline WaveQueue wave_at(const WaveQueue &q, uint64_t off) {
+    WaveQueue r;
+    r.p = q.p ? q.p + off : nullptr;
+    r.v = q.v ? q.v + off : nullptr;
+    r.t = q.t ? q.t + off : nullptr;
+    r.e = q.e ? q.e + off : nullptr;
+    r.h = q.h ? q.h + off : nullptr;
+    return r;
+}
+
+// One hop for the 32 queue slots [base, base + 32) of a warp (slots >= n idle): on hop 0 a
+// slot is a pixel (camera ray from its seed), later a path read from `in`. Paths that go on
+// are appended to `out` with one atomic on `out_count` per warp; paths that end add their
+// sample to the canvas (render.cl:20-26). Every lane of the warp calls this together.
+template <int R>
+__device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, uint32_t n, bool first_hop,
+                                           bool last_hop, uint32_t W, uint32_t H, uint32_t flags,
+                                           float4 *__restrict__ canvas, uint32_t *__restrict__ seeds,
+                                           const WaveQueue &in, const WaveQueue &out, uint32_t *out_count,
+                                           LaneStats &st) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t i = base + lane;
+    bool cont = false;
+    typename PathOf<R>::T ray;
+    uint32_t rng = 0, prev_hash = HASH_NEVER, pixel = 0;
+    Col intensity = {1.0f, 1.0f, 1.0f};
+    Col emission = {0.0f, 0.0f, 0.0f};
+    if (i < n) {
+        if (first_hop) {
+            pixel = i;
+            float px, py, size;
+            pixel_pos(i % W, i / W, W, H, px, py, size);
+            rng = seeds[i];
+            ray = camera<R>(s, px, py, size, rng, flags);
+        } else {
+            ray = path_load<R>(in.p[i], in.v[i]);
+            const float4 t = in.t[i], e = in.e[i];
+            intensity.x = t.x; intensity.y = t.y; intensity.z = t.z;
+            rng = __float_as_uint(t.w);
+            emission.x = e.x; emission.y = e.y; emission.z = e.z;
+            pixel = __float_as_uint(e.w);
+            prev_hash = in.h[i];
+        }
+        bool hit;
+        st.hops += 1;
+        st.tests += s.n;
+        const bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact);
+        st.hits += hit ? 1 : 0;
+        cont = go && !last_hop;
+        if (!cont) {
+            st.samples += 1;
+            float4 c = canvas[pixel];
+            c.x += emission.x; c.y += emission.y; c.z += emission.z; c.w += 1.0f;
+            canvas[pixel] = c;
+            seeds[pixel] = rng;
+        }
+    }
+    const uint32_t want = __ballot_sync(0xffffffffu, cont);
+    if (want) {
+        const int leader = __ffs(want) - 1;
+        uint32_t obase = 0;
+        if (lane == (uint32_t)leader) obase = atomicAdd(out_count, (uint32_t)__popc(want));
+        obase = __shfl_sync(0xffffffffu, obase, leader);
+        if (cont) {
+            const uint32_t j = obase + __popc(want & ((1u << lane) - 1u));
+            path_store<R>(&out.p[j], &out.v[j], ray);
+            out.t[j] = make_float4(intensity.x, intensity.y, intensity.z, __uint_as_float(rng));
+            out.e[j] = make_float4(emission.x, emission.y, emission.z, __uint_as_float(pixel));
+            out.h[j] = prev_hash;
+        }
+    }
+}
+
 // ctr[0]: slots taken by warps of this launch; ctr[1]: paths appended to `out`.
 // in_count: paths in `in` (NULL for hop 0, which covers the W*H pixels).
 template <int R>
@@ -401,63 +498,15 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
 
     const uint32_t lane = threadIdx.x & 31;
     const bool last = hop_index + 1 >= hops;
-    uint32_t n_samples = 0, n_hops = 0, n_hits = 0, n_exact = 0;
+    LaneStats st;
     for (;;) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&ctr[0], 32u);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
-        const uint32_t i = base + lane;
-        bool cont = false;
-        typename PathOf<R>::T ray;
-        uint32_t rng = 0, prev_hash = HASH_NEVER, pixel = 0;
-        Col intensity = {1.0f, 1.0f, 1.0f};
-        Col emission = {0.0f, 0.0f, 0.0f};
-        if (i < n) {
-            if (!in_count) {
-                pixel = i;
-                float px, py, size;
-                pixel_pos(i % W, i / W, W, H, px, py, size);
-                rng = seeds[i];
-                ray = camera<R>(s, px, py, size, rng, flags);
-            } else {
-                ray = path_load<R>(in.p[i], in.v[i]);
-                const float4 t = in.t[i], e = in.e[i];
-                intensity.x = t.x; intensity.y = t.y; intensity.z = t.z;
-                rng = __float_as_uint(t.w);
-                emission.x = e.x; emission.y = e.y; emission.z = e.z;
-                pixel = __float_as_uint(e.w);
-                prev_hash = in.h[i];
-            }
-            bool hit;
-            n_hops += 1;
-            const bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
-            n_hits += hit ? 1 : 0;
-            cont = go && !last;
-            if (!cont) {   // the path ends: this pass's sample of the pixel (render.cl:20-26)
-                n_samples += 1;
-                float4 c = canvas[pixel];
-                c.x += emission.x; c.y += emission.y; c.z += emission.z; c.w += 1.0f;
-                canvas[pixel] = c;
-                seeds[pixel] = rng;
-            }
-        }
-        const uint32_t want = __ballot_sync(0xffffffffu, cont);
-        if (want) {
-            const int leader = __ffs(want) - 1;
-            uint32_t obase = 0;
-            if (lane == (uint32_t)leader) obase = atomicAdd(&ctr[1], (uint32_t)__popc(want));
-            obase = __shfl_sync(0xffffffffu, obase, leader);
-            if (cont) {
-                const uint32_t j = obase + __popc(want & ((1u << lane) - 1u));
-                path_store<R>(&out.p[j], &out.v[j], ray);
-                out.t[j] = make_float4(intensity.x, intensity.y, intensity.z, __uint_as_float(rng));
-                out.e[j] = make_float4(emission.x, emission.y, emission.z, __uint_as_float(pixel));
-                out.h[j] = prev_hash;
-            }
-        }
+        wave_chunk<R>(s, base, n, in_count == nullptr, last, W, H, flags, canvas, seeds, in, out, &ctr[1], st);
     }
-    flush_stats(stats, n_samples, n_hops, n_hits, n_exact, s.n);
+    flush_lane_stats(stats, st);
 }
 
 // ============================================================================ batch
@@ -478,6 +527,7 @@ struct BatchView {          // device copy of htc_view plus host-derived fields
     int32_t address_width;
     uint32_t passes;
     uint32_t max_objects;   // objects the scene buffer can hold
+    uint64_t qoff;          // first slot of the view's region in the wavefront queues
 };
 struct BatchTile { uint32_t view, first, count; };
 
@@ -552,6 +602,127 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
         }
     }
     rewind_queue(queue);
+}
+
+// Wavefront form of the batch: one launch per (pass, hop depth) over every view. Each view
+// has its own region of the two queues and its own append counter; the launch cuts the
+// views' current paths into tiles of `tile_slots` (a block-wide prefix sum over the views'
+// counts, expensive views first), blocks take tiles from a counter and stage a view's scene
+// only when it changes, and warps take 32 slots of the tile at a time (wave_chunk). A
+// view's paths therefore run exactly as in render_wave, and every view's canvas and seeds
+// are bit-identical to rendering it alone.
+//   cnt[h * n_views + v]: paths of view v appended by hop h of this pass;
+//   cnt[hops_max * n_views + h]: tiles taken by blocks of the hop-h launch.
+__device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_t vi, uint32_t pass, uint32_t h,
+                                                     const uint32_t *cnt, uint32_t n_views) {
+    if (pass >= v.passes || h >= v.hops) return 0;
+    if (h == 0) return v.width * v.height;
+    return *reinterpret_cast<const volatile uint32_t *>(&cnt[(h - 1) * n_views + vi]);
+}
+
+__global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
+    const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
+    uint32_t hops_max, uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in,
+    WaveQueue out, uint32_t *cnt, uint64_t *stats, uint32_t *err) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_tile, s_next, s_total;
+    __shared__ int s_staged_view, s_staged_ok;
+    float4 *s_inv = smem;
+    float4 *s_bound = smem + 2 * smem_objects;
+    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * smem_objects);
+    uint32_t *s_pref = s_shape + smem_objects + 4;   // n_order + 1 tile offsets
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+
+    // tiles of every view at this hop, in `order`, as a prefix sum
+    for (uint32_t i = tid; i < n_order; i += blockDim.x) {
+        const uint32_t vi = order[i];
+        const uint32_t n = batch_wave_count(views[vi], vi, pass, h, cnt, n_views);
+        s_pref[i + 1] = (n + tile_slots - 1) / tile_slots;
+    }
+    if (tid == 0) {
+        s_pref[0] = 0;
+        s_staged_view = -1;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        uint32_t carry = 0;
+        for (uint32_t b0 = 0; b0 < n_order; b0 += 32) {
+            const uint32_t i = b0 + lane;
+            uint32_t x = i < n_order ? s_pref[i + 1] : 0;
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+                if (lane >= (uint32_t)off) x += y;
+            }
+            if (i < n_order) s_pref[i + 1] = x + carry;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) s_total = carry;
+    }
+    __syncthreads();
+    const uint32_t total = s_total;
+    StagedScene s;
+    s.n = 0;
+    LaneStats st;
+    uint32_t *grab = &cnt[hops_max * n_views + h];
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            s_tile = total ? atomicAdd(grab, 1u) : 0u;
+            s_next = 0;
+        }
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t >= total) break;
+        uint32_t lo = 0, hi = n_order - 1;   // the last view whose first tile is <= t
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (s_pref[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const uint32_t vi = order[lo];
+        const BatchView &v = views[vi];
+        const uint32_t n = batch_wave_count(v, vi, pass, h, cnt, n_views);
+        const uint32_t first = (t - s_pref[lo]) * tile_slots;
+        const uint32_t count = min(tile_slots, n - first);
+        const int32_t recipe = v.recipe;
+        if ((int)vi != s_staged_view) {
+            bool ok;
+            if (recipe == RECIPE_HY)
+                ok = stage_scene<RECIPE_HY>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
+                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+            else
+                ok = stage_scene<RECIPE_EU>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
+                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+            __syncthreads();
+            if (tid == 0) {
+                s_staged_view = (int)vi;
+                s_staged_ok = ok ? 1 : 0;
+            }
+            __syncthreads();
+        }
+        if (!s_staged_ok) continue;
+        const WaveQueue vin = wave_at(in, v.qoff + first), vout = wave_at(out, v.qoff);
+        const bool first_hop = h == 0, last_hop = h + 1 >= v.hops;
+        uint32_t *out_count = &cnt[h * n_views + vi];
+        float4 *canvas = v.canvas;
+        uint32_t *seeds = v.seeds;
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&s_next, 32u);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= count) break;
+            // slots are pixel numbers on hop 0, tile-relative queue slots later
+            const uint32_t b0 = first_hop ? first + base : base, n0 = first_hop ? first + count : count;
+            if (recipe == RECIPE_HY)
+                wave_chunk<RECIPE_HY>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                                      vout, out_count, st);
+            else
+                wave_chunk<RECIPE_EU>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                                      vout, out_count, st);
+        }
+    }
+    flush_lane_stats(stats, st);
 }
 
 // ============================================================================ post
@@ -1019,6 +1190,7 @@ struct htc_batch {
     uint32_t n_tiles;
     uint32_t smem_objects;
     uint32_t blocks_per_sm;
+    uint32_t tile_pixels;
     int num_sms, max_smem;
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
@@ -1031,6 +1203,14 @@ struct htc_batch {
     size_t p_tiles_cap[2];
     cudaEvent_t staged[2];
     int slot;
+    // wavefront form: view order (expensive first), queues, counters
+    uint32_t *d_order;
+    uint32_t *p_order[2];
+    uint32_t n_views, n_order, hops_max, passes_max;
+    void *wave_buf;
+    uint64_t wave_slots;     // slots per queue
+    uint32_t *d_wcnt;
+    size_t wcnt_words;
 };
 
 static void batch_free(htc_batch *b) {
@@ -1042,7 +1222,11 @@ static void batch_free(htc_batch *b) {
         }
         if (b->p_views[i]) cudaFreeHost(b->p_views[i]);
         if (b->p_tiles[i]) cudaFreeHost(b->p_tiles[i]);
+        if (b->p_order[i]) cudaFreeHost(b->p_order[i]);
     }
+    if (b->d_order) cudaFree(b->d_order);
+    if (b->wave_buf) cudaFree(b->wave_buf);
+    if (b->d_wcnt) cudaFree(b->d_wcnt);
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_views);
@@ -1052,7 +1236,39 @@ static void batch_free(htc_batch *b) {
     delete b;
 }
 
+static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
+    if (b->n_order == 0) return HTC_OK;
+    const size_t smem = smem_bytes(b->smem_objects) + sizeof(uint32_t) * ((size_t)b->n_views + 1);
+    int per_sm = 0;
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch_wave, 128, smem));
+    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
+    if (per_sm < 1) per_sm = 1;
+    const unsigned blocks = (unsigned)per_sm * (unsigned)b->num_sms;
+    WaveQueue q[2];
+    for (int k = 0; k < 2; ++k) {
+        uint8_t *base = reinterpret_cast<uint8_t *>(b->wave_buf) + (size_t)k * WAVE_SLOT_BYTES * b->wave_slots;
+        const uint64_t n = b->wave_slots;
+        q[k].p = reinterpret_cast<float4 *>(base);
+        q[k].v = q[k].p + n;
+        q[k].t = q[k].v + n;
+        q[k].e = q[k].t + n;
+        q[k].h = reinterpret_cast<uint32_t *>(q[k].e + n);
+    }
+    const size_t words = (size_t)(b->n_views + 1) * b->hops_max;
+    for (uint32_t pass = 0; pass < b->passes_max; ++pass) {
+        HTC_CUDA(cudaMemsetAsync(b->d_wcnt, 0, sizeof(uint32_t) * words, st));
+        for (uint32_t h = 0; h < b->hops_max; ++h) {
+            render_batch_wave<<<blocks, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, b->hops_max,
+                                                         pass, h, b->tile_pixels, b->smem_objects, q[(h + 1) & 1],
+                                                         q[h & 1], b->d_wcnt, stats, b->d_err);
+        }
+        HTC_CUDA(cudaGetLastError());
+    }
+    return HTC_OK;
+}
+
 static int batch_launch(htc_batch *b, uint64_t *stats, cudaStream_t st) {
+    if (HT_BATCH_MODE == 2) return batch_launch_wave(b, stats, st);
     if (b->n_tiles == 0) return HTC_OK;
     const size_t smem = smem_bytes(b->smem_objects);
     int per_sm = 0;
@@ -1084,16 +1300,20 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_views, sizeof(BatchView) * max_views);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * max_tiles);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_order, sizeof(uint32_t) * max_views);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
         e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_views[i]), sizeof(BatchView) * max_views, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_order[i]), sizeof(uint32_t) * max_views, cudaHostAllocDefault);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) {
         b->max_smem -= 1024;
         e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(render_batch_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
     }
     if (e != cudaSuccess) {
         batch_free(b);
@@ -1146,9 +1366,19 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
         // shortens the tail of the persistent launch)
         order.push_back({(double)v.passes * v.light_hops * (1.0 + d.max_objects), i});
     }
-    if (smem_bytes(smem_objects) > (size_t)b->max_smem)
+    if (smem_bytes(smem_objects) + sizeof(uint32_t) * ((size_t)n_views + 1) > (size_t)b->max_smem)
         return fail(HTC_ERR_UNSUPPORTED, "a view has more objects than shared memory can stage");
     std::stable_sort(order.begin(), order.end(), [](const std::pair<double, uint32_t> &a, const std::pair<double, uint32_t> &c) { return a.first > c.first; });
+    // wavefront queues: one region of W*H slots (rounded to 64: 16-byte aligned arrays) per view
+    uint64_t slots = 0;
+    uint32_t hops_max = 0, passes_max = 0;
+    for (const auto &o : order) {
+        BatchView &d = b->h_views[o.second];
+        d.qoff = slots;
+        slots += ((uint64_t)d.width * d.height + 63) & ~(uint64_t)63;
+        hops_max = std::max(hops_max, d.hops);
+        passes_max = std::max(passes_max, d.passes);
+    }
     for (const auto &o : order) {
         const BatchView &d = b->h_views[o.second];
         const uint32_t total = d.width * d.height;
@@ -1160,7 +1390,33 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     b->n_tiles = (uint32_t)b->h_tiles.size();
     b->smem_objects = smem_objects;
     b->blocks_per_sm = blocks_per_sm;
+    b->tile_pixels = tile_pixels;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (HT_BATCH_MODE == 2) {
+        // Grow the queues and counters when this set needs more; launches already enqueued on
+        // `stream` may still use the old ones, so they finish first.
+        const size_t words = (size_t)(n_views + 1) * hops_max;
+        if (slots > b->wave_slots || words > b->wcnt_words) HTC_CUDA(cudaStreamSynchronize(st));
+        if (slots > b->wave_slots) {
+            if (b->wave_buf) HTC_CUDA(cudaFree(b->wave_buf));
+            b->wave_buf = nullptr;
+            b->wave_slots = 0;
+            const uint64_t cap = slots + slots / 4;
+            HTC_CUDA(cudaMalloc(&b->wave_buf, 2 * WAVE_SLOT_BYTES * cap));
+            b->wave_slots = cap;
+        }
+        if (words > b->wcnt_words) {
+            if (b->d_wcnt) HTC_CUDA(cudaFree(b->d_wcnt));
+            b->d_wcnt = nullptr;
+            b->wcnt_words = 0;
+            HTC_CUDA(cudaMalloc(&b->d_wcnt, sizeof(uint32_t) * words));
+            b->wcnt_words = words;
+        }
+    }
+    b->n_views = n_views;
+    b->n_order = (uint32_t)order.size();
+    b->hops_max = hops_max;
+    b->passes_max = passes_max;
     // Asynchronous upload through the next pinned slot: wait only for that slot's previous
     // copy, then copy on `stream` (ordered after any launch still reading the device arrays).
     const int k = b->slot;
@@ -1174,6 +1430,8 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
         b->p_tiles_cap[k] = cap;
     }
     if (n_views) std::memcpy(b->p_views[k], b->h_views.data(), sizeof(BatchView) * n_views);
+    for (uint32_t i = 0; i < b->n_order; ++i) b->p_order[k][i] = order[i].second;
+    if (b->n_order) HTC_CUDA(cudaMemcpyAsync(b->d_order, b->p_order[k], sizeof(uint32_t) * b->n_order, cudaMemcpyHostToDevice, st));
     if (b->n_tiles) std::memcpy(b->p_tiles[k], b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles);
     if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->p_views[k], sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
     if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->p_tiles[k], sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));

@@ -27,7 +27,7 @@ def _requests(n=12, rate=400.0, seed=9):
     return out
 
 
-@pytest.mark.parametrize("budget", [120 << 30, 300_000])
+@pytest.mark.parametrize("budget", [120 << 30, 2_000_000])
 def test_served_equals_alone(built, budget):
     ctx = P.Context(0)
     reqs = _requests()
