@@ -124,6 +124,7 @@ struct StagedScene {
     const float4 *inv;       // shared, 2 per object
     const uint32_t *shape;   // shared
     const float4 *bound;     // shared, 1 per object: world-space form for distance bounds
+    const float *mag;        // shared, 1 per object: BOUND_EPS * max |bound component|
     const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials)
     uint32_t n;
     float fov;
@@ -230,6 +231,22 @@ constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
 constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
 constexpr float HORO_M = 1e-3f;      // relative margin of the horosphere root bounds
 
+// Hardware approximations (PTX rcp / sqrt / lg2 / ex2 .approx, relative error near 2^-22) for
+// the bound arithmetic only: every quantity they produce carries a margin of at least 1e-6
+// relative (the threshold itself 1e-2), so they never decide a culling the exact values
+// would not allow. The path's own arithmetic (ray maps, shape tests) never uses them.
+HT_D float rcp_approx(float x) { float r; asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+HT_D float sqrt_approx(float x) { float r; asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+HT_D float lg2_approx(float x) { float r; asm("lg2.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+HT_D float ex2_approx(float x) { float r; asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+constexpr float LN2F = 0.693147180559945f, LOG2EF = 1.442695040888963f;
+
+// Error allowance of F for one object: BOUND_EPS * max |rec component|, so that
+// eF = mag * (|p|^2 + |x| + |y| + 1) >= BOUND_EPS * sum of |terms| of F (one multiply per object).
+HT_D float bound_mag(float4 rec) {
+    return BOUND_EPS * fmaxf(fmaxf(fabsf(rec.x), fabsf(rec.y)), fmaxf(fabsf(rec.z), fabsf(rec.w)));
+}
+
 struct Cull { float S, E, T; };   // sinh, exp, tanh of the threshold; S = E = inf, T = 1: none
 
 // World-space bound record of one object from its f32 map M, in FP64 (once per launch).
@@ -265,6 +282,8 @@ HT_D float4 stage_bound(const Mo &m, uint32_t shape) {
 // Per-hop constants of the bound evaluation.
 struct BoundRay {
     float x, y, t, r2, pv, vx, vy, vz, ax, ay;
+    float K;    // |p|^2 + |x| + |y| + 1: eF = mag * K
+    float Kw;   // t (2 |p.v| + |vx| + |vy|): the part of eW that scales with mag
 };
 HT_D bool cull_point_ok(Q4 p) {
     return p.z >= 0x1p-20f && p.z <= 0x1p20f && fabsf(p.x) + fabsf(p.y) <= 0x1p10f * p.z &&
@@ -277,14 +296,24 @@ HT_D BoundRay bound_ray(Q4 p, Q4 v) {
     b.pv = fmaf(p.x, v.x, fmaf(p.y, v.y, p.z * v.z));
     b.vx = v.x; b.vy = v.y; b.vz = v.z;
     b.ax = fabsf(p.x); b.ay = fabsf(p.y);
+    b.K = b.r2 + b.ax + b.ay + 1.0f;
+    b.Kw = b.t * (2.0f * fabsf(b.pv) + fabsf(b.vx) + fabsf(b.vy));
     return b;
 }
+// eF and eW of one object (the bounds of the float error of F and W)
+HT_D float bound_eF(float mag, const BoundRay &r) { return mag * r.K; }
+HT_D float bound_eW(float mag, float eF, float W, const BoundRay &r) {
+    return fmaf(mag, r.Kw, fmaf(eF, fabsf(r.vz), BOUND_EPS * fabsf(W)));
+}
+// S, E, T are upper bounds of sinh, exp, tanh of the threshold: E from ex2.approx raised by
+// 1e-5 relative (more than its error plus the rounding of thr * log2(e) for thr < 89, above
+// which it is +inf), S and T increasing functions of it.
 HT_D Cull cull_from_dist(float d) {
     const float thr = fmaf(d, 1.0f + CULL_REL, CULL_ABS);
     Cull c;
-    c.S = sinhf(thr);
-    c.E = expf(thr);
-    c.T = tanhf(thr);
+    c.E = ex2_approx(thr * LOG2EF) * (1.0f + 1e-5f);
+    c.S = 0.5f * (c.E - rcp_approx(c.E));
+    c.T = 1.0f - 2.0f * rcp_approx(fmaf(c.E, c.E, 1.0f));
     return c;
 }
 HT_D Cull cull_none() {
@@ -294,23 +323,22 @@ HT_D Cull cull_none() {
     return c;
 }
 // Cheap bound: the distance from the ray start to the object alone (any hit lies on it).
-HT_D bool culled_point(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
+HT_D bool culled_point(float4 rec, float mag, uint32_t shape, const BoundRay &r, const Cull &c) {
     const float t = r.t;
     const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-    const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+    const float eF = bound_eF(mag, r);
     if (shape == 0) return fabsf(F) - eF > 2.0f * t * c.S;
     return t > c.E * (F + eF) || t * c.E < F - eF;
 }
 
 // true when object `rec` provably cannot be hit nearer than the current threshold
-HT_D bool culled(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
+HT_D bool culled(float4 rec, float mag, uint32_t shape, const BoundRay &r, const Cull &c) {
     const float t = r.t;
     const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-    const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+    const float eF = bound_eF(mag, r);
     const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
     const float W = fmaf(t, G, -F * r.vz);
-    const float eW = fmaf(BOUND_EPS * t, fmaf(2.0f * fabsf(rec.x), fabsf(r.pv), fmaf(fabsf(rec.y), fabsf(r.vx), fabsf(rec.z * r.vy))),
-                          eF * fabsf(r.vz) + BOUND_EPS * fabsf(W));
+    const float eW = bound_eW(mag, eF, W, r);
     if (shape == 0) {
         const float Fa = fabsf(F) - eF;       // lower bound of |2 t a|
         const float Wlo = fabsf(W) - eW, Whi = fabsf(W) + eW;
@@ -336,7 +364,7 @@ HT_D bool culled(float4 rec, uint32_t shape, const BoundRay &r, const Cull &c) {
         const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
         if (R2hi < -HORO_M * t * t) return true;        // no crossing
         if (R2lo < HORO_M * t * t) return false;        // nearly tangent: test exactly
-        const float Rlo = sqrtf(R2lo) * (1.0f - 1e-6f), Rhi = sqrtf(R2hi) * (1.0f + 1e-6f);   // r t
+        const float Rlo = sqrt_approx(R2lo) * (1.0f - 1e-6f), Rhi = sqrt_approx(R2hi) * (1.0f + 1e-6f);   // r t
         // margin of the reference's own root test: 2 EPS plus its float error
         const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
         const bool r1 = !(Wlo * t + Rlo * Flo > tol);   // root 1 may be reported
@@ -358,17 +386,17 @@ HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, u
     const float t = r.t;
     for (uint32_t k = 0; k < n; ++k) {   // warp-uniform: broadcast loads
         const float4 rec = s.bound[k];
+        const float mag = s.mag[k];
         const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-        const float eF = BOUND_EPS * fmaf(fabsf(rec.x), r.r2, fmaf(fabsf(rec.y), r.ax, fmaf(fabsf(rec.z), r.ay, fabsf(rec.w))));
+        const float eF = bound_eF(mag, r);
         const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
         const float W = fmaf(t, G, -F * r.vz);
-        const float eW = fmaf(BOUND_EPS * t, fmaf(2.0f * fabsf(rec.x), fabsf(r.pv), fmaf(fabsf(rec.y), fabsf(r.vx), fabsf(rec.z * r.vy))),
-                              eF * fabsf(r.vz) + BOUND_EPS * fabsf(W));
+        const float eW = bound_eW(mag, eF, W, r);
         if (s.shape[k] == 0) {
             if (k == prev_hash) continue;   // a plane is never hit twice in a row
             const float Fa = fabsf(F) - eF, Wlo = fabsf(W) - eW;
             if (!((F > 0.0f) != (W > 0.0f) && Fa > 0.02f * t && Wlo > 0.0f)) continue;
-            const float rr = (fabsf(F) + eF) / Wlo;
+            const float rr = (fabsf(F) + eF) * rcp_approx(Wlo);
             if (rr < 0.99f) best_tanh = fminf(best_tanh, rr);
         } else {
             const float Flo = F - eF, Fhi = F + eF, Wlo = W - eW, Whi = W + eW;
@@ -376,23 +404,24 @@ HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, u
                 const float aWlo = fmaxf(fabsf(W) - eW, 0.0f), aWhi = fabsf(W) + eW;
                 const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
                 if (R2lo > 1e-3f * t * t) {
-                    const float Rlo = sqrtf(R2lo) * (1.0f - 1e-6f), Rhi = sqrtf(R2hi) * (1.0f + 1e-6f);
+                    const float Rlo = sqrt_approx(R2lo) * (1.0f - 1e-6f), Rhi = sqrt_approx(R2hi) * (1.0f + 1e-6f);
                     const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
                     const bool r1 = !(Wlo * t + Rlo * Flo > tol);
                     const bool r2_sure = (Wlo * t - Rhi * Fhi) < -tol - 1e-3f * t * t;
-                    if (!r1 && r2_sure) best_exp = fminf(best_exp, (t + Rhi) / (Flo + Wlo) * 1.001f);
+                    if (!r1 && r2_sure) best_exp = fminf(best_exp, (t + Rhi) * rcp_approx(Flo + Wlo) * 1.001f);
                 }
             } else if (Flo > 1.01f * t && Whi < -0.01f * t) {   // outside, approaching: entry ahead
                 const float aVlo = -Whi / t;
                 const float P = Fhi / t;
                 const float D = 1.0f - P * P + aVlo * aVlo;
-                if (D > 0.02f) best_exp = fminf(best_exp, (Fhi - Wlo) / t / (1.0f + sqrtf(D)));
+                if (D > 0.02f) best_exp = fminf(best_exp, (Fhi - Wlo) * rcp_approx(t * (1.0f + sqrt_approx(D))));
             }
         }
     }
+    // (approximations: every later use adds the threshold's 1e-2 margins)
     float u = __int_as_float(0x7f800000);
-    if (best_tanh < 1.0f) u = atanhf(best_tanh);
-    if (best_exp < __int_as_float(0x7f800000)) u = fminf(u, logf(best_exp));
+    if (best_tanh < 1.0f) u = 0.5f * LN2F * lg2_approx((1.0f + best_tanh) * rcp_approx(1.0f - best_tanh));   // atanh
+    if (best_exp < __int_as_float(0x7f800000)) u = fminf(u, LN2F * lg2_approx(best_exp));
     return u;
 }
 
@@ -417,7 +446,7 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
         uint32_t mask = 0;
         for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads, cheap bound
             const uint32_t k = c0 + j;
-            if (!can_cull || !culled_point(s.bound[k], s.shape[k], br, cull)) mask |= 1u << j;
+            if (!can_cull || !culled_point(s.bound[k], s.mag[k], s.shape[k], br, cull)) mask |= 1u << j;
         }
         if (can_cull) {   // per lane: the ray-aware bound on the survivors only
             uint32_t m = mask;
@@ -425,14 +454,14 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
                 const uint32_t j = __ffs(m) - 1;
                 m &= m - 1;
                 const uint32_t k = c0 + j;
-                if (culled(s.bound[k], s.shape[k], br, cull)) mask &= ~(1u << j);
+                if (culled(s.bound[k], s.mag[k], s.shape[k], br, cull)) mask &= ~(1u << j);
             }
         }
         while (mask) {   // this lane's candidates, in index order
             const uint32_t k = c0 + (__ffs(mask) - 1);
             mask &= mask - 1;
             const uint32_t shape = s.shape[k];
-            if (can_cull && culled_point(s.bound[k], shape, br, cull)) continue;
+            if (can_cull && culled_point(s.bound[k], s.mag[k], shape, br, cull)) continue;
             const bool repeat = (k == prev_hash);
             if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
             ++n_exact;

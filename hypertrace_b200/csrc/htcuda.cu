@@ -76,10 +76,28 @@ struct htc_program {
 // ============================================================================ staging
 // Loads the scene header and the inverse maps / shape indices of every object into shared
 // memory. Returns false (uniformly across the block) when the scene bytes fail validation.
+// Shared-memory layout of a staged scene of up to n objects (smem_bytes(n) bytes): inverse
+// maps (2 float4), bound records (float4), shape indices (u32), bound magnitudes (f32).
+struct SceneSmem {
+    float4 *inv, *bound;
+    uint32_t *shape;
+    float *mag;
+};
+__device__ __forceinline__ SceneSmem carve_scene(float4 *smem, uint32_t n) {
+    SceneSmem c;
+    c.inv = smem;
+    c.bound = smem + 2 * n;
+    c.shape = reinterpret_cast<uint32_t *>(smem + 3 * n);
+    c.mag = reinterpret_cast<float *>(c.shape + n);
+    return c;
+}
+
 template <int R>
 __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t max_objects,
-                            int address_width, uint32_t *err, StagedScene &s, float4 *s_inv,
-                            float4 *s_bound, uint32_t *s_shape, uint32_t *s_hdr) {
+                            int address_width, uint32_t *err, StagedScene &s, const SceneSmem &sm,
+                            uint32_t *s_hdr) {
+    float4 *s_inv = sm.inv, *s_bound = sm.bound;
+    uint32_t *s_shape = sm.shape;
     using L = Layout<R>;
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         uint32_t ok = 1;
@@ -116,11 +134,14 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
             Mo inv = mo_inverse(fwd);
             s_inv[2 * k] = make_float4(inv.a.x, inv.a.y, inv.b.x, inv.b.y);
             s_inv[2 * k + 1] = make_float4(inv.c.x, inv.c.y, inv.d.x, inv.d.y);
-            s_bound[k] = stage_bound(fwd, shape);
+            const float4 rec = stage_bound(fwd, shape);
+            s_bound[k] = rec;
+            sm.mag[k] = bound_mag(rec);
         } else {
             Hom inv = hom3_inverse(load_hom(obj));
             s_inv[2 * k] = make_float4(inv.shift.x, inv.shift.y, inv.shift.z, 0.0f);
             s_inv[2 * k + 1] = make_float4(inv.rot.x, inv.rot.y, inv.rot.z, inv.rot.w);
+            sm.mag[k] = 0.0f;
         }
     }
     const int any_bad = __syncthreads_or(bad ? 1 : 0);
@@ -131,6 +152,7 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
     s.inv = s_inv;
     s.bound = s_bound;
     s.shape = s_shape;
+    s.mag = sm.mag;
     s.objects = scene + L::OBJECTS;
     s.n = n;
     s.fov = ldf(scene, L::FOV);
@@ -194,11 +216,9 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
-    float4 *s_inv = smem;
-    float4 *s_bound = smem + 2 * max_objects;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
+    const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
-    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr)) return;
+    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, sm, s_hdr)) return;
 
     // 128 threads = 32 x 4 pixels: each warp covers 32 consecutive pixels of a row.
     const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -354,11 +374,9 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     uint32_t *queue) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
-    float4 *s_inv = smem;
-    float4 *s_bound = smem + 2 * max_objects;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
+    const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
-    const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr);
+    const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, sm, s_hdr);
     LaneStats st;
     if (staged) trace_pixels<R>(s, &queue[0], 0, W * H, W, H, hops, passes, flags, canvas, seeds, st);
     flush_stats(stats, st.samples, st.hops, st.hits, st.exact, staged ? s.n : 0);
@@ -490,11 +508,9 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
     __shared__ uint32_t s_hdr[2];
     const uint32_t n = in_count ? *reinterpret_cast<const volatile uint32_t *>(in_count) : W * H;
     if (n == 0 || blockIdx.x * 128u >= n) return;   // nothing for this block: skip the staging
-    float4 *s_inv = smem;
-    float4 *s_bound = smem + 2 * max_objects;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * max_objects);
+    const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
-    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, s_inv, s_bound, s_shape, s_hdr)) return;
+    if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, sm, s_hdr)) return;
 
     const uint32_t lane = threadIdx.x & 31;
     const bool last = hop_index + 1 >= hops;
@@ -538,9 +554,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
     __shared__ uint32_t s_hdr[2];
     __shared__ uint32_t s_tile, s_next;
     __shared__ int s_staged_view, s_staged_ok;
-    float4 *s_inv = smem;
-    float4 *s_bound = smem + 2 * smem_objects;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * smem_objects);
+    const SceneSmem sm = carve_scene(smem, smem_objects);
     StagedScene s;
     s.n = 0;
     LaneStats st;
@@ -562,10 +576,10 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
             bool ok;
             if (recipe == RECIPE_HY)
                 ok = stage_scene<RECIPE_HY>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+                                            err, s, sm, s_hdr);
             else
                 ok = stage_scene<RECIPE_EU>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+                                            err, s, sm, s_hdr);
             __syncthreads();
             if (threadIdx.x == 0) {
                 s_staged_view = (int)tile.view;
@@ -628,10 +642,8 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
     __shared__ uint32_t s_hdr[2];
     __shared__ uint32_t s_tile, s_next, s_total;
     __shared__ int s_staged_view, s_staged_ok;
-    float4 *s_inv = smem;
-    float4 *s_bound = smem + 2 * smem_objects;
-    uint32_t *s_shape = reinterpret_cast<uint32_t *>(smem + 3 * smem_objects);
-    uint32_t *s_pref = s_shape + smem_objects + 4;   // n_order + 1 tile offsets
+    const SceneSmem sm = carve_scene(smem, smem_objects);
+    uint32_t *s_pref = reinterpret_cast<uint32_t *>(sm.mag + smem_objects) + 4;   // n_order + 1 tile offsets
     const uint32_t tid = threadIdx.x, lane = tid & 31;
 
     // tiles of every view at this hop, in `order`, as a prefix sum
@@ -690,10 +702,10 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
             bool ok;
             if (recipe == RECIPE_HY)
                 ok = stage_scene<RECIPE_HY>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+                                            err, s, sm, s_hdr);
             else
                 ok = stage_scene<RECIPE_EU>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, s_inv, s_bound, s_shape, s_hdr);
+                                            err, s, sm, s_hdr);
             __syncthreads();
             if (tid == 0) {
                 s_staged_view = (int)vi;
@@ -786,8 +798,8 @@ static int check_program(const htc_program *p) {
     if (!p) return fail(HTC_ERR_INVALID, "program is NULL");
     return HTC_OK;
 }
-static size_t smem_bytes(uint32_t max_objects) {
-    return (size_t)max_objects * 48u + (size_t)max_objects * 4u + 16u;
+static size_t smem_bytes(uint32_t max_objects) {   // carve_scene's layout + 16 bytes
+    return (size_t)max_objects * 56u + 16u;
 }
 static uint32_t objects_capacity(int recipe, size_t scene_size) {
     const size_t hdr = recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
