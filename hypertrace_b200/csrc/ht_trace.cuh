@@ -230,6 +230,10 @@ constexpr float CULL_REL = 1e-2f, CULL_ABS = 1e-2f;
 
 constexpr float BOUND_EPS = 1e-5f;   // relative error allowance of F and W (>> f32 rounding)
 constexpr float HORO_M = 1e-3f;      // relative margin of the horosphere root bounds
+// Objects the upper estimate looks at (the first ones in index order).
+#ifndef HT_EST_OBJECTS
+#define HT_EST_OBJECTS 32u
+#endif
 
 // Hardware approximations (PTX rcp / sqrt / lg2 / ex2 .approx, relative error near 2^-22) for
 // the bound arithmetic only: every quantity they produce carries a margin of at least 1e-6
@@ -332,13 +336,19 @@ HT_D bool culled_point(float4 rec, float mag, uint32_t shape, const BoundRay &r,
 }
 
 // true when object `rec` provably cannot be hit nearer than the current threshold
-HT_D bool culled(float4 rec, float mag, uint32_t shape, const BoundRay &r, const Cull &c) {
-    const float t = r.t;
-    const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-    const float eF = bound_eF(mag, r);
+// F, W of one object along the ray and the bounds of their float error
+struct BoundFW { float F, eF, W, eW; };
+HT_D BoundFW bound_fw(float4 rec, float mag, const BoundRay &r) {
+    BoundFW b;
+    b.F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
+    b.eF = bound_eF(mag, r);
     const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
-    const float W = fmaf(t, G, -F * r.vz);
-    const float eW = bound_eW(mag, eF, W, r);
+    b.W = fmaf(r.t, G, -b.F * r.vz);
+    b.eW = bound_eW(mag, b.eF, b.W, r);
+    return b;
+}
+HT_D bool culled_fw(const BoundFW &b, uint32_t shape, float t, const Cull &c) {
+    const float F = b.F, eF = b.eF, W = b.W, eW = b.eW;
     if (shape == 0) {
         const float Fa = fabsf(F) - eF;       // lower bound of |2 t a|
         const float Wlo = fabsf(W) - eW, Whi = fabsf(W) + eW;
@@ -375,54 +385,57 @@ HT_D bool culled(float4 rec, float mag, uint32_t shape, const BoundRay &r, const
         return (!r1 || r1_far) && (!r2 || r2_far);
     }
 }
+HT_D bool culled(float4 rec, float mag, uint32_t shape, const BoundRay &r, const Cull &c) {
+    return culled_fw(bound_fw(rec, mag, r), shape, r.t, c);
+}
 
-// Upper estimate of the nearest hit among objects [0, n) that the reference surely reports:
-// geodesic planes the ray crosses ahead (tanh of the crossing = |F| / |W|) and horospheres
-// entered ahead from outside or left ahead from inside (e^s of the crossing), with margins
-// far above the float error of either side. +inf when none qualifies. A threshold derived from
-// it (cull_from_dist) then culls before the first exact test.
-HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, uint32_t prev_hash) {
-    float best_tanh = 2.0f, best_exp = __int_as_float(0x7f800000);
-    const float t = r.t;
-    for (uint32_t k = 0; k < n; ++k) {   // warp-uniform: broadcast loads
-        const float4 rec = s.bound[k];
-        const float mag = s.mag[k];
-        const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-        const float eF = bound_eF(mag, r);
-        const float G = fmaf(2.0f * rec.x, r.pv, fmaf(rec.y, r.vx, rec.z * r.vy));
-        const float W = fmaf(t, G, -F * r.vz);
-        const float eW = bound_eW(mag, eF, W, r);
-        if (s.shape[k] == 0) {
-            if (k == prev_hash) continue;   // a plane is never hit twice in a row
-            const float Fa = fabsf(F) - eF, Wlo = fabsf(W) - eW;
-            if (!((F > 0.0f) != (W > 0.0f) && Fa > 0.02f * t && Wlo > 0.0f)) continue;
-            const float rr = (fabsf(F) + eF) * rcp_approx(Wlo);
-            if (rr < 0.99f) best_tanh = fminf(best_tanh, rr);
-        } else {
-            const float Flo = F - eF, Fhi = F + eF, Wlo = W - eW, Whi = W + eW;
-            if (Fhi < 0.999f * t && Flo > 0.0f && (Flo + Wlo) > 0.0f) {   // inside: exit ahead
-                const float aWlo = fmaxf(fabsf(W) - eW, 0.0f), aWhi = fabsf(W) + eW;
-                const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
-                if (R2lo > 1e-3f * t * t) {
-                    const float Rlo = sqrt_approx(R2lo) * (1.0f - 1e-6f), Rhi = sqrt_approx(R2hi) * (1.0f + 1e-6f);
-                    const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
-                    const bool r1 = !(Wlo * t + Rlo * Flo > tol);
-                    const bool r2_sure = (Wlo * t - Rhi * Fhi) < -tol - 1e-3f * t * t;
-                    if (!r1 && r2_sure) best_exp = fminf(best_exp, (t + Rhi) * rcp_approx(Flo + Wlo) * 1.001f);
-                }
-            } else if (Flo > 1.01f * t && Whi < -0.01f * t) {   // outside, approaching: entry ahead
-                const float aVlo = -Whi / t;
-                const float P = Fhi / t;
-                const float D = 1.0f - P * P + aVlo * aVlo;
-                if (D > 0.02f) best_exp = fminf(best_exp, (Fhi - Wlo) * rcp_approx(t * (1.0f + sqrt_approx(D))));
-            }
-        }
+// Upper bound of e^(2 s) at the nearest crossing of one object that the reference surely
+// reports (s = distance along the ray): geodesic planes crossed ahead (tanh s = |F| / |W|,
+// not the plane the ray just left), horospheres entered ahead from outside or left ahead
+// from inside (e^s of the crossing), with margins far above the float error of either side.
+// +inf when the object has no such crossing.
+HT_D float sure_crossing_e2(const BoundFW &b, uint32_t shape, bool plane_repeat, float t) {
+    const float inf = __int_as_float(0x7f800000);
+    const float F = b.F, eF = b.eF, W = b.W, eW = b.eW;
+    if (shape == 0) {
+        if (plane_repeat) return inf;   // a plane is never hit twice in a row
+        const float Fa = fabsf(F) - eF, Wlo = fabsf(W) - eW;
+        if (!((F > 0.0f) != (W > 0.0f) && Fa > 0.02f * t && Wlo > 0.0f)) return inf;
+        const float rr = (fabsf(F) + eF) * rcp_approx(Wlo);   // >= tanh s
+        if (!(rr < 0.99f)) return inf;
+        return (1.0f + rr) * rcp_approx(1.0f - rr);
     }
-    // (approximations: every later use adds the threshold's 1e-2 margins)
-    float u = __int_as_float(0x7f800000);
-    if (best_tanh < 1.0f) u = 0.5f * LN2F * lg2_approx((1.0f + best_tanh) * rcp_approx(1.0f - best_tanh));   // atanh
-    if (best_exp < __int_as_float(0x7f800000)) u = fminf(u, LN2F * lg2_approx(best_exp));
-    return u;
+    const float Flo = F - eF, Fhi = F + eF, Wlo = W - eW, Whi = W + eW;
+    float e = inf;
+    if (Fhi < 0.999f * t && Flo > 0.0f && (Flo + Wlo) > 0.0f) {   // inside: exit ahead
+        const float aWlo = fmaxf(fabsf(W) - eW, 0.0f), aWhi = fabsf(W) + eW;
+        const float R2lo = t * t - Fhi * Fhi + aWlo * aWlo, R2hi = t * t - Flo * Flo + aWhi * aWhi;
+        if (R2lo > 1e-3f * t * t) {
+            const float Rlo = sqrt_approx(R2lo) * (1.0f - 1e-6f), Rhi = sqrt_approx(R2hi) * (1.0f + 1e-6f);
+            const float tol = 2e-6f * Fhi * Fhi + 1e-5f * (aWhi * t + Rhi * Fhi);
+            const bool r1 = !(Wlo * t + Rlo * Flo > tol);
+            const bool r2_sure = (Wlo * t - Rhi * Fhi) < -tol - 1e-3f * t * t;
+            if (!r1 && r2_sure) e = (t + Rhi) * rcp_approx(Flo + Wlo) * 1.001f;
+        }
+    } else if (Flo > 1.01f * t && Whi < -0.01f * t) {   // outside, approaching: entry ahead
+        const float it = rcp_approx(t);
+        const float aVlo = -Whi * it, P = Fhi * it;
+        const float D = 1.0f - P * P + aVlo * aVlo;
+        if (D > 0.02f) e = (Fhi - Wlo) * it * rcp_approx(1.0f + sqrt_approx(D));
+    }
+    return e * e;
+}
+// Distance of a crossing from its e^(2 s) bound (the threshold built from it adds 1e-2 margins).
+HT_D float dist_from_e2(float x) { return 0.5f * LN2F * lg2_approx(x); }
+
+// Upper estimate of the nearest hit among objects [0, n) that the reference surely reports
+// (the least sure_crossing_e2), +inf when none qualifies. A threshold derived from it
+// (cull_from_dist) then culls before the first exact test.
+HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, uint32_t prev_hash) {
+    float best = __int_as_float(0x7f800000);
+    for (uint32_t k = 0; k < n; ++k)   // warp-uniform: broadcast loads
+        best = fminf(best, sure_crossing_e2(bound_fw(s.bound[k], s.mag[k], r), s.shape[k], k == prev_hash, r.t));
+    return best < __int_as_float(0x7f800000) ? dist_from_e2(best) : best;
 }
 
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
@@ -438,7 +451,7 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const BoundRay br = bound_ray(p, v);
     Cull cull = cull_none();
     if (can_cull) {   // a threshold before the first exact test, from the first chunk's crossings
-        const float u = upper_estimate(s, min(32u, s.n), br, prev_hash);
+        const float u = upper_estimate(s, min(HT_EST_OBJECTS, s.n), br, prev_hash);
         if (u < __int_as_float(0x7f800000)) cull = cull_from_dist(u);
     }
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
