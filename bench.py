@@ -35,7 +35,7 @@ UNIT = "Msamples/s"
 # Executed FP32 operations per unit of work in the CUDA path (static tally of the source,
 # each add/sub/mul/div/sqrt/log/sin/cos = 1): see DESIGN.md "Roofline".
 FLOPS_PER_EXACT_TEST = 219      # one inverse ray map (204) + shape distance test lower bound (15)
-FLOPS_PER_BOUND_TEST = 18       # world-space distance bound of one object (hops x objects of them)
+FLOPS_PER_BOUND_TEST = 12       # world-space point bound of one object (hops x objects of them)
 FLOPS_PER_HIT_HOP = 936         # winner recompute + map back + interact maps + material
 FLOPS_PER_SAMPLE = 120          # camera ray
 FLOPS_PER_ESTIMATE = 30         # upper estimate of the nearest crossing, per object of the first chunk and hop
