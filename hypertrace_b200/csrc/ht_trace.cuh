@@ -125,6 +125,7 @@ struct StagedScene {
     const uint32_t *shape;   // shared
     const float4 *bound;     // shared, 1 per object: world-space form for distance bounds
     const float *mag;        // shared, 1 per object: BOUND_EPS * max |bound component|
+    float4 *win;             // shared, this thread's 2 float4: the scan winner's local ray
     const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials)
     uint32_t n;
     float fov;
@@ -489,6 +490,8 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
                     min_x = x;
                     kmin = k;
                     cull = cull_from_dist(dist);
+                    s.win[0] = make_float4(l.p.x, l.p.y, l.p.z, l.p.w);   // kept for the hit
+                    s.win[1] = make_float4(l.v.x, l.v.y, l.v.z, l.v.w);
                 }
             }
         }
@@ -505,7 +508,12 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     const uint8_t *obj = s.objects + (size_t)kmin * OBJ_STRIDE;
     const Mo fwd = load_mo(obj);
     const bool repeat = (kmin == prev_hash);
-    HyRay l = ray_hy_map_call(inv, p, v);
+    HyRay l;   // the winner's local ray, as the scan computed it (the same map, the same bits)
+    {
+        const float4 a = s.win[0], b = s.win[1];
+        l.p = q4(a.x, a.y, a.z, a.w);
+        l.v = q4(b.x, b.y, b.z, b.w);
+    }
     HyPath lh;
     Q4 normal;
     if (s.shape[kmin] == 0) plane_hy_hit(l.p, l.v, lh, normal);

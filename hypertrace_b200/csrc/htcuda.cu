@@ -77,18 +77,25 @@ struct htc_program {
 // Loads the scene header and the inverse maps / shape indices of every object into shared
 // memory. Returns false (uniformly across the block) when the scene bytes fail validation.
 // Shared-memory layout of a staged scene of up to n objects (smem_bytes(n) bytes): inverse
-// maps (2 float4), bound records (float4), shape indices (u32), bound magnitudes (f32).
+// maps (2 float4), bound records (float4), shape indices (u32), bound magnitudes (f32) per
+// object, then 2 float4 per thread of a 128-thread block (the scan's winner, local frame).
+constexpr uint32_t BLOCK_THREADS = 128;
 struct SceneSmem {
     float4 *inv, *bound;
     uint32_t *shape;
     float *mag;
+    float4 *win;
+    float4 *end;   // first float4 past the layout
 };
+__host__ __device__ constexpr size_t scene_win_offset(uint32_t n) { return ((size_t)n * 56u + 15u) & ~(size_t)15u; }
 __device__ __forceinline__ SceneSmem carve_scene(float4 *smem, uint32_t n) {
     SceneSmem c;
     c.inv = smem;
     c.bound = smem + 2 * n;
     c.shape = reinterpret_cast<uint32_t *>(smem + 3 * n);
     c.mag = reinterpret_cast<float *>(c.shape + n);
+    c.win = smem + scene_win_offset(n) / 16;
+    c.end = c.win + 2 * BLOCK_THREADS;
     return c;
 }
 
@@ -153,6 +160,7 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
     s.bound = s_bound;
     s.shape = s_shape;
     s.mag = sm.mag;
+    s.win = sm.win + 2 * tid;
     s.objects = scene + L::OBJECTS;
     s.n = n;
     s.fov = ldf(scene, L::FOV);
@@ -643,7 +651,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
     __shared__ uint32_t s_tile, s_next, s_total;
     __shared__ int s_staged_view, s_staged_ok;
     const SceneSmem sm = carve_scene(smem, smem_objects);
-    uint32_t *s_pref = reinterpret_cast<uint32_t *>(sm.mag + smem_objects) + 4;   // n_order + 1 tile offsets
+    uint32_t *s_pref = reinterpret_cast<uint32_t *>(sm.end);   // n_order + 1 tile offsets
     const uint32_t tid = threadIdx.x, lane = tid & 31;
 
     // tiles of every view at this hop, in `order`, as a prefix sum
@@ -798,8 +806,8 @@ static int check_program(const htc_program *p) {
     if (!p) return fail(HTC_ERR_INVALID, "program is NULL");
     return HTC_OK;
 }
-static size_t smem_bytes(uint32_t max_objects) {   // carve_scene's layout + 16 bytes
-    return (size_t)max_objects * 56u + 16u;
+static size_t smem_bytes(uint32_t max_objects) {   // carve_scene's layout
+    return scene_win_offset(max_objects) + 2u * 16u * BLOCK_THREADS;
 }
 static uint32_t objects_capacity(int recipe, size_t scene_size) {
     const size_t hdr = recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
