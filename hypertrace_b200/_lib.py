@@ -60,6 +60,7 @@ SIGNATURES = [
     ("htc_gamma", _i, [_u32, _u32, _f, _vp, _vp, _vp]),
     ("htc_pack", _i, [_u32, _u32, _vp, _vp, _vp]),
     ("htc_extract_gamma_pack", _i, [_u32, _u32, _u32, _f, _vp, _vp, _vp]),
+    ("htc_fill_seeds", _i, [_vp, _u32, _u32, _u32, _vp]),
     ("htc_fp32_probe", _i, [_vp, _u32, _i, ctypes.POINTER(ctypes.c_double), _vp]),
     ("htc_batch_create", _i, [_u32, _u32, ctypes.POINTER(_vp)]),
     ("htc_batch_destroy", None, [_vp]),
@@ -68,6 +69,7 @@ SIGNATURES = [
     ("htc_batch_graph_launch", _i, [_vp, _vp, _vp]),
     ("htc_batch_check", _i, [_vp, _vp]),
     ("htc_batch_tile_count", _i, [_vp, ctypes.POINTER(_u32)]),
+    ("htc_batch_reserve", _i, [_vp, ctypes.c_uint64, _u32, _vp]),
 ]
 
 

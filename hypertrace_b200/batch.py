@@ -96,6 +96,10 @@ class BatchRenderer:
     def check(self) -> None:
         _lib.call("htc_batch_check", self.handle, self.ctx.stream())
 
+    def reserve(self, pixels: int, max_hops: int) -> None:
+        """Size the wavefront queues for view sets of up to `pixels` pixels and `max_hops` hops."""
+        _lib.call("htc_batch_reserve", self.handle, pixels, max_hops, self.ctx.stream())
+
     def tile_count(self) -> int:
         n = ctypes.c_uint32()
         _lib.call("htc_batch_tile_count", self.handle, ctypes.byref(n))
@@ -134,8 +138,8 @@ def config3(seed: int = 0x5EED0003, n_views: int = 96, spp_scale: float = 1.0) -
 
 
 def autotune(renderer: BatchRenderer, views: Sequence[View], passes: int = 1,
-             tiles: Sequence[int] = (512, 1024, 2048, 4096, 8192),
-             residency: Sequence[int] = (4, 5, 6)) -> Tuple[int, int, dict]:
+             tiles: Sequence[int] = (256, 512, 1024, 2048),
+             residency: Sequence[int] = (5, 6, 7)) -> Tuple[int, int, dict]:
     """Times one launch of `passes` passes per candidate (tile size x blocks per SM) on the
     views themselves and returns the fastest (tile_pixels, blocks_per_sm, timings). The
     canvases and seeds are restored afterwards, so tuning leaves no trace in the results."""

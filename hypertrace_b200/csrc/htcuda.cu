@@ -53,6 +53,10 @@ thread_local std::string g_last_error;
 #ifndef HT_BATCH_MODE
 #define HT_BATCH_MODE 2
 #endif
+// Batched wavefronts: 1 = one launch per recipe for each (pass, hop depth), 0 = one launch for both.
+#ifndef HT_BATCH_SPLIT
+#define HT_BATCH_SPLIT 1
+#endif
 
 // Device error word bits.
 constexpr uint32_t ERR_SCENE = 1u;
@@ -634,7 +638,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
 // view's paths therefore run exactly as in render_wave, and every view's canvas and seeds
 // are bit-identical to rendering it alone.
 //   cnt[h * n_views + v]: paths of view v appended by hop h of this pass;
-//   cnt[hops_max * n_views + h]: tiles taken by blocks of the hop-h launch.
+//   grab: tiles taken by the blocks of one launch (a word of its own per launch of a pass).
 __device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_t vi, uint32_t pass, uint32_t h,
                                                      const uint32_t *cnt, uint32_t n_views) {
     if (pass >= v.passes || h >= v.hops) return 0;
@@ -642,28 +646,46 @@ __device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_
     return *reinterpret_cast<const volatile uint32_t *>(&cnt[(h - 1) * n_views + vi]);
 }
 
-__global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
+// RF = 0 serves views of either recipe (a runtime branch per tile); RF = RECIPE_HY or
+// RECIPE_EU compiles one recipe only (its views alone in `order`), with fewer registers.
+template <int RF>
+__global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) render_batch_wave(
     const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
-    uint32_t hops_max, uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in,
-    WaveQueue out, uint32_t *cnt, uint64_t *stats, uint32_t *err) {
+    uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
+    uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
-    __shared__ uint32_t s_tile, s_next, s_total;
+    __shared__ uint32_t s_tile, s_next, s_total, s_tsize;
     __shared__ int s_staged_view, s_staged_ok;
     const SceneSmem sm = carve_scene(smem, smem_objects);
     uint32_t *s_pref = reinterpret_cast<uint32_t *>(sm.end);   // n_order + 1 tile offsets
     const uint32_t tid = threadIdx.x, lane = tid & 31;
 
-    // tiles of every view at this hop, in `order`, as a prefix sum
+    // tiles of every view at this hop, in `order`, as a prefix sum. The tile size adapts to
+    // the launch: about 16 tiles per block when the paths are few (a multiple of 128 slots,
+    // so the four warps of a block take equal shares; at least one chunk per warp),
+    // `tile_slots` when they are many, so a launch ends with short tiles.
     for (uint32_t i = tid; i < n_order; i += blockDim.x) {
         const uint32_t vi = order[i];
-        const uint32_t n = batch_wave_count(views[vi], vi, pass, h, cnt, n_views);
-        s_pref[i + 1] = (n + tile_slots - 1) / tile_slots;
+        s_pref[i + 1] = batch_wave_count(views[vi], vi, pass, h, cnt, n_views);
     }
     if (tid == 0) {
         s_pref[0] = 0;
         s_staged_view = -1;
     }
+    __syncthreads();
+    if (tid < 32) {
+        uint64_t paths = 0;
+        for (uint32_t i = lane; i < n_order; i += 32) paths += s_pref[i + 1];
+        for (int off = 16; off > 0; off >>= 1) paths += __shfl_xor_sync(0xffffffffu, paths, off);
+        uint64_t per = (paths / (16ull * gridDim.x) + 127) & ~127ull;
+        if (per < 128) per = 128;
+        if (per > tile_slots) per = tile_slots;
+        if (lane == 0) s_tsize = (uint32_t)per;
+    }
+    __syncthreads();
+    const uint32_t tile = s_tsize;
+    for (uint32_t i = tid; i < n_order; i += blockDim.x) s_pref[i + 1] = (s_pref[i + 1] + tile - 1) / tile;
     __syncthreads();
     if (tid < 32) {
         uint32_t carry = 0;
@@ -684,7 +706,6 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
     StagedScene s;
     s.n = 0;
     LaneStats st;
-    uint32_t *grab = &cnt[hops_max * n_views + h];
     for (;;) {
         __syncthreads();
         if (tid == 0) {
@@ -703,9 +724,9 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch_wave(
         const uint32_t vi = order[lo];
         const BatchView &v = views[vi];
         const uint32_t n = batch_wave_count(v, vi, pass, h, cnt, n_views);
-        const uint32_t first = (t - s_pref[lo]) * tile_slots;
-        const uint32_t count = min(tile_slots, n - first);
-        const int32_t recipe = v.recipe;
+        const uint32_t first = (t - s_pref[lo]) * tile;
+        const uint32_t count = min(tile, n - first);
+        const int32_t recipe = RF ? RF : v.recipe;
         if ((int)vi != s_staged_view) {
             bool ok;
             if (recipe == RECIPE_HY)
@@ -775,6 +796,22 @@ __global__ void k_pack(uint32_t n, const float4 *__restrict__ in, uchar4 *__rest
         out[i] = make_uchar4(pack1(c.x), pack1(c.y), pack1(c.z), pack1(c.w));
     }
 }
+// Per-pixel initial RNG states: seed_i = fmix32(global_seed ^ fmix32(i + offset)), MurmurHash3's
+// 32-bit finaliser (the harness seeds; the reference fills the buffer from a host SmallRng,
+// processing/src/canvas.rs:193-195, and its kernel only consumes it).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+__global__ void k_fill_seeds(uint32_t n, uint32_t global_seed, uint32_t offset, uint32_t *__restrict__ seeds) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        seeds[i] = fmix32(global_seed ^ fmix32(i + offset));
+}
+
 __global__ void k_extract_gamma_pack(uint32_t n, float passes, float g, const float4 *__restrict__ canvas,
                                      uchar4 *__restrict__ out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1198,6 +1235,14 @@ int htc_extract_gamma_pack(uint32_t W, uint32_t H, uint32_t passes, float gamma,
     return HTC_OK;
 }
 
+int htc_fill_seeds(uint32_t *seeds, uint32_t n, uint32_t global_seed, uint32_t offset, void *stream) {
+    if (!seeds && n) return fail(HTC_ERR_INVALID, "seeds is NULL");
+    if (n == 0) return HTC_OK;
+    k_fill_seeds<<<post_blocks(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(n, global_seed, offset, seeds);
+    HTC_CUDA(cudaGetLastError());
+    return HTC_OK;
+}
+
 // ---------------------------------------------------------------- batches
 }  // extern "C"
 
@@ -1226,7 +1271,7 @@ struct htc_batch {
     // wavefront form: view order (expensive first), queues, counters
     uint32_t *d_order;
     uint32_t *p_order[2];
-    uint32_t n_views, n_order, hops_max, passes_max;
+    uint32_t n_views, n_order, n_hy, n_eu, hops_max, passes_max;
     void *wave_buf;
     uint64_t wave_slots;     // slots per queue
     uint32_t *d_wcnt;
@@ -1256,14 +1301,19 @@ static void batch_free(htc_batch *b) {
     delete b;
 }
 
+template <int RF>
+static int batch_wave_blocks(htc_batch *b, size_t smem, unsigned *blocks) {
+    int per_sm = 0;
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch_wave<RF>, 128, smem));
+    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
+    if (per_sm < 1) per_sm = 1;
+    *blocks = (unsigned)per_sm * (unsigned)b->num_sms;
+    return HTC_OK;
+}
+
 static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
     if (b->n_order == 0) return HTC_OK;
     const size_t smem = smem_bytes(b->smem_objects) + sizeof(uint32_t) * ((size_t)b->n_views + 1);
-    int per_sm = 0;
-    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch_wave, 128, smem));
-    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
-    if (per_sm < 1) per_sm = 1;
-    const unsigned blocks = (unsigned)per_sm * (unsigned)b->num_sms;
     WaveQueue q[2];
     for (int k = 0; k < 2; ++k) {
         uint8_t *base = reinterpret_cast<uint8_t *>(b->wave_buf) + (size_t)k * WAVE_SLOT_BYTES * b->wave_slots;
@@ -1274,13 +1324,33 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
         q[k].e = q[k].t + n;
         q[k].h = reinterpret_cast<uint32_t *>(q[k].e + n);
     }
-    const size_t words = (size_t)(b->n_views + 1) * b->hops_max;
+    unsigned blocks_any = 0, blocks_hy = 0, blocks_eu = 0;
+    int rc = HT_BATCH_SPLIT ? batch_wave_blocks<RECIPE_HY>(b, smem, &blocks_hy) : batch_wave_blocks<0>(b, smem, &blocks_any);
+    if (!rc && HT_BATCH_SPLIT) rc = batch_wave_blocks<RECIPE_EU>(b, smem, &blocks_eu);
+    if (rc) return rc;
+    const size_t words = (size_t)(b->n_views + 3) * b->hops_max;
+    uint32_t *grab = b->d_wcnt + (size_t)b->n_views * b->hops_max;   // 3 words per hop depth
+    const uint32_t *order_hy = b->d_order + b->n_order, *order_eu = order_hy + b->n_hy;
     for (uint32_t pass = 0; pass < b->passes_max; ++pass) {
         HTC_CUDA(cudaMemsetAsync(b->d_wcnt, 0, sizeof(uint32_t) * words, st));
         for (uint32_t h = 0; h < b->hops_max; ++h) {
-            render_batch_wave<<<blocks, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, b->hops_max,
-                                                         pass, h, b->tile_pixels, b->smem_objects, q[(h + 1) & 1],
-                                                         q[h & 1], b->d_wcnt, stats, b->d_err);
+            const WaveQueue &in = q[(h + 1) & 1], &out = q[h & 1];
+            if (!HT_BATCH_SPLIT) {
+                render_batch_wave<0><<<blocks_any, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, pass,
+                                                                   h, b->tile_pixels, b->smem_objects, in, out,
+                                                                   b->d_wcnt, grab + 3 * h, stats, b->d_err);
+                continue;
+            }
+            if (b->n_hy)
+                render_batch_wave<RECIPE_HY><<<blocks_hy, 128, smem, st>>>(b->d_views, order_hy, b->n_hy, b->n_views,
+                                                                           pass, h, b->tile_pixels, b->smem_objects, in,
+                                                                           out, b->d_wcnt, grab + 3 * h + 1, stats,
+                                                                           b->d_err);
+            if (b->n_eu)
+                render_batch_wave<RECIPE_EU><<<blocks_eu, 128, smem, st>>>(b->d_views, order_eu, b->n_eu, b->n_views,
+                                                                           pass, h, b->tile_pixels, b->smem_objects, in,
+                                                                           out, b->d_wcnt, grab + 3 * h + 2, stats,
+                                                                           b->d_err);
         }
         HTC_CUDA(cudaGetLastError());
     }
@@ -1320,20 +1390,24 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_views, sizeof(BatchView) * max_views);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * max_tiles);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_order, sizeof(uint32_t) * max_views);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_order, 2 * sizeof(uint32_t) * max_views);   // all, then by recipe
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
         e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_views[i]), sizeof(BatchView) * max_views, cudaHostAllocDefault);
-        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_order[i]), sizeof(uint32_t) * max_views, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_order[i]), 2 * sizeof(uint32_t) * max_views, cudaHostAllocDefault);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) {
         b->max_smem -= 1024;
         e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(render_batch_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+            e = cudaFuncSetAttribute(render_batch_wave<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(render_batch_wave<RECIPE_HY>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(render_batch_wave<RECIPE_EU>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
     }
     if (e != cudaSuccess) {
         batch_free(b);
@@ -1344,6 +1418,41 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
 }
 
 void htc_batch_destroy(htc_batch *b) { batch_free(b); }
+
+}  // extern "C"
+
+// Grows the wavefront queues (slots per queue) and counters (words) when a view set needs
+// more; launches already enqueued on `st` may still use the old ones, so they finish first.
+static int batch_grow(htc_batch *b, uint64_t slots, size_t words, cudaStream_t st) {
+    if (slots <= b->wave_slots && words <= b->wcnt_words) return HTC_OK;
+    HTC_CUDA(cudaStreamSynchronize(st));
+    if (slots > b->wave_slots) {
+        if (b->wave_buf) HTC_CUDA(cudaFree(b->wave_buf));
+        b->wave_buf = nullptr;
+        b->wave_slots = 0;
+        const uint64_t cap = (slots + slots / 4 + 63) & ~(uint64_t)63;
+        HTC_CUDA(cudaMalloc(&b->wave_buf, 2 * WAVE_SLOT_BYTES * cap));
+        b->wave_slots = cap;
+    }
+    if (words > b->wcnt_words) {
+        if (b->d_wcnt) HTC_CUDA(cudaFree(b->d_wcnt));
+        b->d_wcnt = nullptr;
+        b->wcnt_words = 0;
+        HTC_CUDA(cudaMalloc(&b->d_wcnt, sizeof(uint32_t) * words));
+        b->wcnt_words = words;
+    }
+    return HTC_OK;
+}
+
+extern "C" {
+
+int htc_batch_reserve(htc_batch *b, uint64_t pixels, uint32_t max_hops, void *stream) {
+    if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
+    if (max_hops == 0) return fail(HTC_ERR_INVALID, "max_hops must be positive");
+    // each view's region is rounded up to 64 slots
+    return batch_grow(b, pixels + 64ull * b->max_views, (size_t)(b->max_views + 3) * max_hops,
+                      reinterpret_cast<cudaStream_t>(stream));
+}
 
 int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, uint32_t tile_pixels,
                         uint32_t blocks_per_sm, void *stream) {
@@ -1399,7 +1508,8 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
         hops_max = std::max(hops_max, d.hops);
         passes_max = std::max(passes_max, d.passes);
     }
-    for (const auto &o : order) {
+    for (const auto &o : order) {   // tiles of the persistent batch kernel only
+        if (HT_BATCH_MODE != 1) break;
         const BatchView &d = b->h_views[o.second];
         const uint32_t total = d.width * d.height;
         for (uint32_t first = 0; first < total; first += tile_pixels) {
@@ -1413,25 +1523,8 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     b->tile_pixels = tile_pixels;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (HT_BATCH_MODE == 2) {
-        // Grow the queues and counters when this set needs more; launches already enqueued on
-        // `stream` may still use the old ones, so they finish first.
-        const size_t words = (size_t)(n_views + 1) * hops_max;
-        if (slots > b->wave_slots || words > b->wcnt_words) HTC_CUDA(cudaStreamSynchronize(st));
-        if (slots > b->wave_slots) {
-            if (b->wave_buf) HTC_CUDA(cudaFree(b->wave_buf));
-            b->wave_buf = nullptr;
-            b->wave_slots = 0;
-            const uint64_t cap = slots + slots / 4;
-            HTC_CUDA(cudaMalloc(&b->wave_buf, 2 * WAVE_SLOT_BYTES * cap));
-            b->wave_slots = cap;
-        }
-        if (words > b->wcnt_words) {
-            if (b->d_wcnt) HTC_CUDA(cudaFree(b->d_wcnt));
-            b->d_wcnt = nullptr;
-            b->wcnt_words = 0;
-            HTC_CUDA(cudaMalloc(&b->d_wcnt, sizeof(uint32_t) * words));
-            b->wcnt_words = words;
-        }
+        int rc = batch_grow(b, slots, (size_t)(n_views + 3) * hops_max, st);
+        if (rc) return rc;
     }
     b->n_views = n_views;
     b->n_order = (uint32_t)order.size();
@@ -1450,8 +1543,15 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
         b->p_tiles_cap[k] = cap;
     }
     if (n_views) std::memcpy(b->p_views[k], b->h_views.data(), sizeof(BatchView) * n_views);
-    for (uint32_t i = 0; i < b->n_order; ++i) b->p_order[k][i] = order[i].second;
-    if (b->n_order) HTC_CUDA(cudaMemcpyAsync(b->d_order, b->p_order[k], sizeof(uint32_t) * b->n_order, cudaMemcpyHostToDevice, st));
+    // the cost order of every view, then the same order split by recipe
+    uint32_t *po = b->p_order[k];
+    b->n_hy = b->n_eu = 0;
+    for (uint32_t i = 0; i < b->n_order; ++i) po[i] = order[i].second;
+    for (uint32_t i = 0; i < b->n_order; ++i)
+        if (b->h_views[order[i].second].recipe == RECIPE_HY) po[b->n_order + b->n_hy++] = order[i].second;
+    for (uint32_t i = 0; i < b->n_order; ++i)
+        if (b->h_views[order[i].second].recipe != RECIPE_HY) po[b->n_order + b->n_hy + b->n_eu++] = order[i].second;
+    if (b->n_order) HTC_CUDA(cudaMemcpyAsync(b->d_order, po, 2 * sizeof(uint32_t) * b->n_order, cudaMemcpyHostToDevice, st));
     if (b->n_tiles) std::memcpy(b->p_tiles[k], b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles);
     if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->p_views[k], sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
     if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->p_tiles[k], sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));

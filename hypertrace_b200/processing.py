@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .scene import Scene, pixel_seeds, serialize
+from .scene import Scene, serialize
 
 
 @dataclasses.dataclass
@@ -71,9 +71,9 @@ class Canvas:
         self.shape = (w, h)
         self.context = context
         self.image = torch.zeros(h * w * 4, dtype=torch.float32, device=context.device)
-        seeds = pixel_seeds(global_seed, w * h)
-        host = torch.from_numpy(seeds.view(np.int32).copy()).pin_memory()
-        self.seeds = host.to(context.device, non_blocking=True)   # ordered on the current stream
+        # pixel_seeds(global_seed, w * h), computed on the device (ordered on the current stream)
+        self.seeds = torch.empty(w * h, dtype=torch.int32, device=context.device)
+        _lib.call("htc_fill_seeds", self.seeds.data_ptr(), w * h, global_seed & 0xFFFFFFFF, 0, context.stream())
         self.passes = 0
 
     @property

@@ -1,11 +1,13 @@
 """Continuous-batching render server.
 
 Requests arrive over time (Poisson). Admitted requests keep their canvas, RNG seeds and
-scene on the device until they finish; every step is ONE batched launch (htc_batch_*) over
-all admitted requests, so requests that arrive while others render join the next step and
-their work overlaps on the GPU. Two classes: interactive frames (all their passes in the
-next step, admitted first) and batch jobs (a quantum of passes per step). Admission is
-bounded by an HBM budget; what does not fit waits on the host.
+scene on the device until they finish; every step is ONE batched render (htc_batch_*: a
+launch per pass, hop depth and recipe, each over every view of the step) over the admitted
+requests, so requests that arrive while others render join the next step and their work
+overlaps on the GPU. Two classes: interactive frames (all their passes in the next step,
+admitted first) and batch jobs (a quantum of passes per step). Admission is bounded by an
+HBM budget (what does not fit waits on the host) and allocates at most a few requests per
+loop turn, so that a burst of arrivals does not hold the next step back.
 
 Results are bit-identical to rendering each request alone (each pixel keeps its RNG stream
 and sample order), which tests/test_gpu_serve.py checks in a mixed run.
@@ -96,6 +98,10 @@ class Server:
         self.budget = hbm_budget_bytes
         self.step_samples = step_samples    # work of one step: bounds the wait of a new arrival
         self.renderer = BatchRenderer(ctx, max_views=4096, max_tiles=1 << 21)
+        # queues for the largest step (its views cover at most step_samples pixels, plus one
+        # oversized job), so that set_views never has to grow them mid-run
+        self.renderer.reserve(min(step_samples + 1920 * 1080, hbm_budget_bytes // 136), 8)
+        self.admit_per_step = 4             # allocations per loop turn: spreads the host work
         self.tile_pixels = tile_pixels
         self.blocks_per_sm = blocks_per_sm
         self.gamma = gamma
@@ -176,14 +182,16 @@ class Server:
                 ai += 1
             # admission: interactive first, then batch jobs, while the HBM budget allows;
             # a request larger than the whole budget can never run and is refused
+            admits = 0
             for q in (waiting_i, waiting):
                 while q and q[0].view.device_bytes() > self.budget:
                     r = q.popleft()
                     r.refused = True
                     done += 1
-                while q and used + q[0].view.device_bytes() <= self.budget:
+                while q and admits < self.admit_per_step and used + q[0].view.device_bytes() <= self.budget:
                     r = q.popleft()
                     r.view.allocate(self.ctx)
+                    admits += 1
                     r.admitted = time.perf_counter() - t0
                     used += r.view.device_bytes()
                     active.append(r)

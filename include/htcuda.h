@@ -189,13 +189,20 @@ void htc_batch_destroy(htc_batch *batch);
  * copied (two calls back). */
 int htc_batch_set_views(htc_batch *batch, const htc_view *views, uint32_t n_views,
                         uint32_t tile_pixels, uint32_t blocks_per_sm, void *stream);
-/* One launch rendering every view's `passes`. stats as in htc_render_passes. */
+/* Sizes the batch's wavefront queues (2 x 68 bytes per pixel) for view sets of up to `pixels`
+ * pixels in total and up to `max_hops` light hops, so that htc_batch_set_views need not grow
+ * them (growing waits for the launches already enqueued on `stream`). */
+int htc_batch_reserve(htc_batch *batch, uint64_t pixels, uint32_t max_hops, void *stream);
+/* Renders every view's `passes`: one launch per pass index, hop depth and recipe over all the
+ * views (wavefronts). stats as in htc_render_passes. */
 int htc_batch_render(htc_batch *batch, uint64_t *stats, void *stream);
 /* The same launch through a CUDA graph captured on first use (re-captured after
  * htc_batch_set_views); `stats` is baked into the graph at capture. */
 int htc_batch_graph_launch(htc_batch *batch, uint64_t *stats, void *stream);
 /* Reads and clears the batch's device error word (synchronises `stream`). */
 int htc_batch_check(htc_batch *batch, void *stream);
+/* Tiles the last htc_batch_set_views cut for a persistent launch; the wavefront form (the
+ * default) cuts its tiles on the device at every launch and reports 0. */
 int htc_batch_tile_count(const htc_batch *batch, uint32_t *n_tiles);
 
 /* ---------------------------------------------------------------- post chain
@@ -211,6 +218,13 @@ int htc_pack(uint32_t width, uint32_t height, const float *image, uint8_t *packe
  * processing/src/pipeline.rs:53-62). */
 int htc_extract_gamma_pack(uint32_t width, uint32_t height, uint32_t passes, float gamma,
                            const float *canvas, uint8_t *packed, void *stream);
+
+/* Initial per-pixel RNG states seeds[i] = fmix32(global_seed ^ fmix32(i + offset)) (MurmurHash3's
+ * 32-bit finaliser), written on the device. The reference fills its seed buffer from a host
+ * SmallRng stream (processing/src/canvas.rs:193-195) and its kernel only reads it; these are
+ * the seeds every test and benchmark of this library uses (hypertrace_b200.scene.pixel_seeds
+ * computes the same values on the host). */
+int htc_fill_seeds(uint32_t *seeds, uint32_t n, uint32_t global_seed, uint32_t offset, void *stream);
 
 /* ---------------------------------------------------------------- calibration
  * FP32 FMA throughput probe used as the roofline denominator of the render kernels

@@ -79,6 +79,13 @@ def test_persistent_equals_repeated_plain(built, cfg):
     assert np.array_equal(cv_a.view(np.uint32), cv_b.view(np.uint32))
 
 
+@pytest.mark.parametrize("W,H,seed", [(1, 1, 0), (33, 7, 5), (1920, 1080, 0xDEADBEEF), (640, 480, 0xFFFFFFFF)])
+def test_device_seeds_equal_host_seeds(built, W, H, seed):
+    """Canvas seeds come from htc_fill_seeds on the device; they equal scene.pixel_seeds."""
+    canvas = P.Canvas(P.Context(0), (W, H), global_seed=seed)
+    assert np.array_equal(canvas.seeds.cpu().numpy().view(np.uint32), S.pixel_seeds(seed, W * H))
+
+
 @pytest.mark.parametrize("cfg,W,H,passes", [("config0", 160, 120, 5), ("config1", 200, 150, 3),
                                            ("config2", 480, 270, 2), ("config1", 33, 7, 4)])
 def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes):
