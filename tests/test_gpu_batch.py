@@ -72,3 +72,28 @@ def test_batch_autotune_restores_state(built):
     assert (tile, res) in t and len(t) == 4
     for v, s in zip(views, snap):
         assert torch.equal(v.canvas.seeds, s)
+
+
+def test_batch_large_views_adaptive_tiles(built):
+    """Views large enough that launches pick tiles above 128 slots (two 1920x1080 views and a
+    small one), queues sized by htc_batch_reserve: equal to each view rendered alone."""
+    def make():
+        return [B.View(S.hyperbolic_scene(30, 45, 6.0, 8, 77, camera=S.random_moebius(np.random.default_rng(3), 1.0)),
+                       1920, 1080, 2, 901),
+                B.View(S.euclidean_scene(8, 4, 78, camera=B.random_hom3(np.random.default_rng(4))), 1920, 1080, 2, 902),
+                B.View(S.hyperbolic_scene(5, 7, 5.0, 8, 79), 96, 40, 2, 903)]
+    ctx = P.Context(0)
+    views, alone = make(), make()
+    for v in views + alone:
+        v.allocate(ctx)
+    br = B.BatchRenderer(ctx, max_views=8, max_tiles=16)
+    br.reserve(2 * 1920 * 1080 + 96 * 40, 8)
+    br.set_views(views, [2, 2, 2], tile_pixels=2048, blocks_per_sm=0)
+    br.render()
+    br.check()
+    for v in alone:
+        P.Render(ctx, v.scene.recipe, v.scene.hops).render_passes(v.buffer, v.canvas, 2)
+    torch.cuda.synchronize()
+    for a, b in zip(views, alone):
+        assert torch.equal(a.canvas.seeds, b.canvas.seeds)
+        assert torch.equal(a.canvas.image.view(torch.int32), b.canvas.image.view(torch.int32))
