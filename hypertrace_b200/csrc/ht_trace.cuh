@@ -458,6 +458,9 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
         const uint32_t cn = min(32u, s.n - c0);
         uint32_t mask = 0;
+        // kept rolled: the kernel is bound by instruction fetch as much as by issue (unrolled
+        // by 8: 7.06 ms per pass at 1080p / 200 objects, fully: 9.43, rolled: 6.24)
+#pragma unroll 1
         for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads, cheap bound
             const uint32_t k = c0 + j;
             if (!can_cull || !culled_point(s.bound[k], s.mag[k], s.shape[k], br, cull)) mask |= 1u << j;
