@@ -449,7 +449,10 @@ __host__ __device__ inline WaveQueue wave_at(const WaveQueue &q, uint64_t off) {
 // slot is a pixel (camera ray from its seed), later a path read from `in`. Paths that go on
 // are appended to `out` with one atomic on `out_count` per warp; paths that end add their
 // sample to the canvas (render.cl:20-26). Every lane of the warp calls this together.
-template <int R>
+// FH: 1 = hop 0 (pixels), 2 = a later hop (queue), known at compile time so that each
+// kernel carries only its own half (the kernel is bound by instruction fetch as much as by
+// issue); 0 = decided by `first_hop` at run time.
+template <int R, int FH>
 __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, uint32_t n, bool first_hop,
                                            bool last_hop, uint32_t W, uint32_t H, uint32_t flags,
                                            float4 *__restrict__ canvas, uint32_t *__restrict__ seeds,
@@ -462,8 +465,9 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
     uint32_t rng = 0, prev_hash = HASH_NEVER, pixel = 0;
     Col intensity = {1.0f, 1.0f, 1.0f};
     Col emission = {0.0f, 0.0f, 0.0f};
+    const bool first = FH == 1 || (FH == 0 && first_hop);
     if (i < n) {
-        if (first_hop) {
+        if (first) {
             pixel = i;
             float px, py, size;
             pixel_pos(i % W, i / W, W, H, px, py, size);
@@ -510,7 +514,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
 
 // ctr[0]: slots taken by warps of this launch; ctr[1]: paths appended to `out`.
 // in_count: paths in `in` (NULL for hop 0, which covers the W*H pixels).
-template <int R>
+template <int R, int FH>
 __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
     uint32_t W, uint32_t H, uint32_t hops, uint32_t hop_index, uint32_t flags, float4 *__restrict__ canvas,
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
     WaveQueue out, uint32_t *ctr) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2];
-    const uint32_t n = in_count ? *reinterpret_cast<const volatile uint32_t *>(in_count) : W * H;
+    const uint32_t n = FH == 1 ? W * H : *reinterpret_cast<const volatile uint32_t *>(in_count);
     if (n == 0 || blockIdx.x * 128u >= n) return;   // nothing for this block: skip the staging
     const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
@@ -532,7 +536,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
         if (lane == 0) base = atomicAdd(&ctr[0], 32u);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
-        wave_chunk<R>(s, base, n, in_count == nullptr, last, W, H, flags, canvas, seeds, in, out, &ctr[1], st);
+        wave_chunk<R, FH>(s, base, n, FH == 1, last, W, H, flags, canvas, seeds, in, out, &ctr[1], st);
     }
     flush_lane_stats(stats, st);
 }
@@ -648,7 +652,7 @@ __device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_
 
 // RF = 0 serves views of either recipe (a runtime branch per tile); RF = RECIPE_HY or
 // RECIPE_EU compiles one recipe only (its views alone in `order`), with fewer registers.
-template <int RF>
+template <int RF, int FH>
 __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) render_batch_wave(
     const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
     uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
@@ -744,7 +748,7 @@ __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) ren
         }
         if (!s_staged_ok) continue;
         const WaveQueue vin = wave_at(in, v.qoff + first), vout = wave_at(out, v.qoff);
-        const bool first_hop = h == 0, last_hop = h + 1 >= v.hops;
+        const bool first_hop = FH == 1, last_hop = h + 1 >= v.hops;
         uint32_t *out_count = &cnt[h * n_views + vi];
         float4 *canvas = v.canvas;
         uint32_t *seeds = v.seeds;
@@ -756,10 +760,10 @@ __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) ren
             // slots are pixel numbers on hop 0, tile-relative queue slots later
             const uint32_t b0 = first_hop ? first + base : base, n0 = first_hop ? first + count : count;
             if (recipe == RECIPE_HY)
-                wave_chunk<RECIPE_HY>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                wave_chunk<RECIPE_HY, FH>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
                                       vout, out_count, st);
             else
-                wave_chunk<RECIPE_EU>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                wave_chunk<RECIPE_EU, FH>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
                                       vout, out_count, st);
         }
     }
@@ -857,7 +861,8 @@ template <int R>
 static int set_smem_attr(size_t smem) {
     HTC_CUDA(cudaFuncSetAttribute(render_plain<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HTC_CUDA(cudaFuncSetAttribute(render_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    HTC_CUDA(cudaFuncSetAttribute(render_wave<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HTC_CUDA(cudaFuncSetAttribute(render_wave<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HTC_CUDA(cudaFuncSetAttribute(render_wave<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return HTC_OK;
 }
 
@@ -1113,7 +1118,7 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
                        uint32_t max_objects, size_t smem, float4 *cv, uint32_t *seeds, uint32_t passes,
                        uint64_t *stats, cudaStream_t st) {
     int per_sm = 0;
-    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_wave<R>, 128, smem));
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_wave<R, 2>, 128, smem));
     if (per_sm < 1) per_sm = 1;
     uint64_t blocks = (uint64_t)per_sm * (uint64_t)p->num_sms;
     const uint64_t needed = ((uint64_t)W * H + 127) / 128;
@@ -1125,7 +1130,7 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
         for (uint32_t h = 0; h < p->hops; ++h) {
             const WaveQueue in = h == 0 ? none : q[(h - 1) & 1];
             const uint32_t *in_count = h == 0 ? nullptr : p->d_wave_ctr + 2 * (h - 1) + 1;
-            render_wave<R><<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+            (h == 0 ? render_wave<R, 1> : render_wave<R, 2>)<<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
                                                                p->hops, h, p->flags, cv, seeds, stats, p->d_err, in,
                                                                in_count, q[h & 1], p->d_wave_ctr + 2 * h);
         }
@@ -1302,9 +1307,16 @@ static void batch_free(htc_batch *b) {
 }
 
 template <int RF>
+static cudaError_t batch_wave_smem_attr(int smem) {
+    cudaError_t e = cudaFuncSetAttribute(render_batch_wave<RF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(render_batch_wave<RF, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
+template <int RF>
 static int batch_wave_blocks(htc_batch *b, size_t smem, unsigned *blocks) {
     int per_sm = 0;
-    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch_wave<RF>, 128, smem));
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch_wave<RF, 2>, 128, smem));
     if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
     if (per_sm < 1) per_sm = 1;
     *blocks = (unsigned)per_sm * (unsigned)b->num_sms;
@@ -1336,18 +1348,18 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
         for (uint32_t h = 0; h < b->hops_max; ++h) {
             const WaveQueue &in = q[(h + 1) & 1], &out = q[h & 1];
             if (!HT_BATCH_SPLIT) {
-                render_batch_wave<0><<<blocks_any, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, pass,
+                (h == 0 ? render_batch_wave<0, 1> : render_batch_wave<0, 2>)<<<blocks_any, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, pass,
                                                                    h, b->tile_pixels, b->smem_objects, in, out,
                                                                    b->d_wcnt, grab + 3 * h, stats, b->d_err);
                 continue;
             }
             if (b->n_hy)
-                render_batch_wave<RECIPE_HY><<<blocks_hy, 128, smem, st>>>(b->d_views, order_hy, b->n_hy, b->n_views,
+                (h == 0 ? render_batch_wave<RECIPE_HY, 1> : render_batch_wave<RECIPE_HY, 2>)<<<blocks_hy, 128, smem, st>>>(b->d_views, order_hy, b->n_hy, b->n_views,
                                                                            pass, h, b->tile_pixels, b->smem_objects, in,
                                                                            out, b->d_wcnt, grab + 3 * h + 1, stats,
                                                                            b->d_err);
             if (b->n_eu)
-                render_batch_wave<RECIPE_EU><<<blocks_eu, 128, smem, st>>>(b->d_views, order_eu, b->n_eu, b->n_views,
+                (h == 0 ? render_batch_wave<RECIPE_EU, 1> : render_batch_wave<RECIPE_EU, 2>)<<<blocks_eu, 128, smem, st>>>(b->d_views, order_eu, b->n_eu, b->n_views,
                                                                            pass, h, b->tile_pixels, b->smem_objects, in,
                                                                            out, b->d_wcnt, grab + 3 * h + 2, stats,
                                                                            b->d_err);
@@ -1403,11 +1415,9 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
         b->max_smem -= 1024;
         e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(render_batch_wave<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(render_batch_wave<RECIPE_HY>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(render_batch_wave<RECIPE_EU>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
+            e = batch_wave_smem_attr<0>(b->max_smem);
+        if (e == cudaSuccess) e = batch_wave_smem_attr<RECIPE_HY>(b->max_smem);
+        if (e == cudaSuccess) e = batch_wave_smem_attr<RECIPE_EU>(b->max_smem);
     }
     if (e != cudaSuccess) {
         batch_free(b);

@@ -97,3 +97,27 @@ def test_batch_large_views_adaptive_tiles(built):
     for a, b in zip(views, alone):
         assert torch.equal(a.canvas.seeds, b.canvas.seeds)
         assert torch.equal(a.canvas.image.view(torch.int32), b.canvas.image.view(torch.int32))
+
+
+def test_batch_mixed_hop_counts(built):
+    """Views of 1, 2, 3 and 5 light hops in one batch (hop-depth launches past a view's H find
+    no paths of it): each equal to the view rendered alone."""
+    def make():
+        return [B.View(S.hyperbolic_scene(6, 9, 5.0, 1, 61), 70, 30, 3, 701),
+                B.View(S.euclidean_scene(5, 2, 62), 40, 40, 2, 702),
+                B.View(S.hyperbolic_scene(12, 15, 5.0, 5, 63), 50, 66, 4, 703),
+                B.View(S.euclidean_scene(3, 3, 64), 33, 17, 1, 704)]
+    ctx = P.Context(0)
+    views, alone = make(), make()
+    for v in views + alone:
+        v.allocate(ctx)
+    br = B.BatchRenderer(ctx, max_views=8, max_tiles=16)
+    br.set_views(views, [v.spp for v in views], tile_pixels=512)
+    br.render(graph=True)
+    br.check()
+    for v in alone:
+        P.Render(ctx, v.scene.recipe, v.scene.hops).render_passes(v.buffer, v.canvas, v.spp)
+    torch.cuda.synchronize()
+    for a, b in zip(views, alone):
+        assert torch.equal(a.canvas.seeds, b.canvas.seeds)
+        assert torch.equal(a.canvas.image.view(torch.int32), b.canvas.image.view(torch.int32))
