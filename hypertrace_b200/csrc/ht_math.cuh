@@ -156,8 +156,8 @@ HT_D HyRay ray_hy_map(const Mo &m, Q4 p, Q4 v) {
     if (bad) return ray_hy_map_ieee(m, p, v);
     return o;
 }
-// The same map, out of line: used by the once-per-hop winner path so that only the scan
-// keeps an inlined copy (instruction-cache footprint).
+// The same map, out of line: the object scan and the hit path share this one copy of its
+// code (instruction-cache footprint; an inlined copy in the scan measured slower).
 static __device__ __noinline__ HyRay ray_hy_map_call(const Mo m, const Q4 p, const Q4 v) { return ray_hy_map(m, p, v); }
 
 // Camera map (view/mapped.inl:20-26): direction = mo_apply_dir (one normalize), then start.

@@ -192,7 +192,10 @@ HT_D void horosphere_hit(Q4 p, Q4 d, bool repeat, HyPath &hit, Q4 &normal) {
 
 // Camera ray: view/point/impl.inl:18-25 (hy_origin = j, hyperbolic.cc:4-6) then the
 // camera Moebius map (view/mapped.inl:20-26).
-HT_D HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint32_t &rng, uint32_t flags) {
+// Out of line: once per sample, and keeping its code out of the hop kernel's instruction
+// stream measured 3 % faster at 1920x1080 / 200 objects.
+static __device__ __noinline__ HyPath camera_hy(const StagedScene &s, float px, float py, float size, uint32_t &rng,
+                                                uint32_t flags) {
     float u0 = rng_uniform(rng);
     float u1 = rng_uniform(rng);
     float jx = (flags & FLAG_JITTER_YX) ? u1 : u0;
@@ -482,7 +485,9 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
             const bool repeat = (k == prev_hash);
             if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
             ++n_exact;
-            HyRay l = ray_hy_map(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+            // the out-of-line copy of the map, shared with the hit path: one copy of its code
+            // (the kernel is bound by instruction fetch as much as by issue)
+            HyRay l = ray_hy_map_call(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
             const float x = shape == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, repeat);
             // candidates come in index order, so x above the best's cannot win (its distance
             // is not smaller, and a tie keeps the lower index)
