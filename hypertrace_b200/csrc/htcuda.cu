@@ -185,11 +185,11 @@ __device__ __forceinline__ typename PathOf<R>::T camera(const StagedScene &s, fl
     if constexpr (R == RECIPE_HY) return camera_hy(s, px, py, size, rng, flags);
     else return camera_eu(s, px, py, size, rng, flags);
 }
-template <int R>
+template <int R, bool OOL = true>
 __device__ __forceinline__ bool hop(const StagedScene &s, typename PathOf<R>::T &ray, uint32_t &rng,
                                     uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit,
                                     uint32_t &n_exact) {
-    if constexpr (R == RECIPE_HY) return hop_hy(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
+    if constexpr (R == RECIPE_HY) return hop_hy<OOL>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
     else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
 }
 
@@ -452,7 +452,7 @@ __host__ __device__ inline WaveQueue wave_at(const WaveQueue &q, uint64_t off) {
 // FH: 1 = hop 0 (pixels), 2 = a later hop (queue), known at compile time so that each
 // kernel carries only its own half (the kernel is bound by instruction fetch as much as by
 // issue); 0 = decided by `first_hop` at run time.
-template <int R, int FH>
+template <int R, int FH, bool OOL = true>
 __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, uint32_t n, bool first_hop,
                                            bool last_hop, uint32_t W, uint32_t H, uint32_t flags,
                                            float4 *__restrict__ canvas, uint32_t *__restrict__ seeds,
@@ -485,7 +485,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
         bool hit;
         st.hops += 1;
         st.tests += s.n;
-        const bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact);
+        const bool go = hop<R, OOL>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact);
         st.hits += hit ? 1 : 0;
         cont = go && !last_hop;
         if (!cont) {
@@ -760,10 +760,10 @@ __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) ren
             // slots are pixel numbers on hop 0, tile-relative queue slots later
             const uint32_t b0 = first_hop ? first + base : base, n0 = first_hop ? first + count : count;
             if (recipe == RECIPE_HY)
-                wave_chunk<RECIPE_HY, FH>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                wave_chunk<RECIPE_HY, FH, false>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
                                       vout, out_count, st);
             else
-                wave_chunk<RECIPE_EU, FH>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
+                wave_chunk<RECIPE_EU, FH, false>(s, b0, n0, first_hop, last_hop, v.width, v.height, v.flags, canvas, seeds, vin,
                                       vout, out_count, st);
         }
     }
