@@ -87,7 +87,8 @@ def test_device_seeds_equal_host_seeds(built, W, H, seed):
 
 
 @pytest.mark.parametrize("cfg,W,H,passes", [("config0", 160, 120, 5), ("config1", 200, 150, 3),
-                                           ("config2", 480, 270, 2), ("config1", 33, 7, 4)])
+                                           ("config2", 480, 270, 2), ("config1", 33, 7, 4),
+                                           ("config1", 1, 1, 3), ("config0", 1, 37, 2)])
 def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes):
     """Hop-depth wavefronts over ray-state queues == P plain launches, bit for bit, with the
     same statistics (samples, hops, hits, exact tests)."""
