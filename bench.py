@@ -297,17 +297,22 @@ def main():
     # through the entry point that still uses it, for comparison
     persistent = None
     if rank == 0:
-        stats.zero_()
         status = ctypes.c_uint32(0)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        _lib.call("htc_render_passes_noalloc", sc.recipe, sc.hops, 32, 0, W, H, buf.ptr(), buf.size,
-                  canvas.image.data_ptr(), canvas.seeds.data_ptr(), args.passes, stats.data_ptr(),
-                  ctypes.byref(status), stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        p_ms = []
+        for i in range(3):   # the first call sets the entry point up on this device: untimed
+            stats.zero_()
+            l2_flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.call("htc_render_passes_noalloc", sc.recipe, sc.hops, 32, 0, W, H, buf.ptr(), buf.size,
+                      canvas.image.data_ptr(), canvas.seeds.data_ptr(), args.passes, stats.data_ptr(),
+                      ctypes.byref(status), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i > 0:
+                p_ms.append(e0.elapsed_time(e1))
+        ms = float(np.mean(p_ms))
         ps = stats.cpu().numpy()
         persistent = {"value": float(ps[0]) / ms / 1e3, "unit": UNIT, "ms_per_launch": ms,
                       "ray_bounces_per_s": float(ps[1]) / ms * 1e3, "kernel": "render_persistent"}
@@ -455,12 +460,20 @@ def bench_batched(args):
         vs = B.config3(spp_scale=args.spp_scale)
         ms = 0.0
         renders = {}
+        # each program's wavefront queues, sized once by its largest view, outside the timing
+        for v in sorted(vs, key=lambda v: -v.width * v.height):
+            key = (v.scene.recipe, v.scene.hops)
+            if key not in renders and wavefront:
+                v.allocate(ctx)
+                renders[key] = P.Render(ctx, *key)
+                renders[key].render_wavefront(v.buffer, v.canvas, 1)
+                v.release()
         for v in vs:
             v.allocate(ctx)
             key = (v.scene.recipe, v.scene.hops)
             r = renders.setdefault(key, P.Render(ctx, *key))
             if wavefront:
-                ms += _time_ms(lambda: r.render_passes(v.buffer, v.canvas, v.spp, sync=False), stream)
+                ms += _time_ms(lambda: r.render_wavefront(v.buffer, v.canvas, v.spp, sync=False), stream)
             else:
                 ms += _time_ms(lambda: [r.render(v.buffer, v.canvas, sync=False) for _ in range(v.spp)], stream)
             v.release()

@@ -249,7 +249,9 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
         for (uint32_t i = 0; i < hops; ++i) {
             bool hit;
             n_hops += 1;
-            bool go = hop<R>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
+            // root tests inline: faster for this kernel (per view on the mixed workload's
+            // views, 2138 vs 2177 ms), unlike the wavefront kernel
+            bool go = hop<R, false>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
             n_hits += hit ? 1 : 0;
             if (!go) break;
         }
@@ -1167,8 +1169,14 @@ int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene,
     int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
     if (rc) return rc;
     if (passes == 0) return HTC_OK;
-    if (HT_PASSES_MODE == 2) return htc_render_wavefront(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
-    if (HT_PASSES_MODE == 0) {
+    // Small canvases of cheap scenes run the one-pass kernel: their deeper hop launches would
+    // leave most of the GPU idle (measured per view, 256x256 and 640x480: Euclidean 26.9 vs
+    // 34.6 ms, hyperbolic with fewer than 100 objects 122.7 vs 131.5 ms, one-pass vs
+    // wavefronts). Either way the result is the same bits.
+    const bool cheap = (uint64_t)W * H < (1u << 19) && (p->recipe == HTC_RECIPE_EU || max_objects < 100);
+    if (HT_PASSES_MODE == 2 && !cheap)
+        return htc_render_wavefront(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
+    if (HT_PASSES_MODE == 0 || HT_PASSES_MODE == 2) {
         for (uint32_t k = 0; k < passes; ++k) {
             int rc2 = htc_render_ex(p, W, H, scene, scene_size, canvas, seeds, stats, stream);
             if (rc2) return rc2;

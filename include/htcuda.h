@@ -122,7 +122,9 @@ int htc_render(htc_program *program, uint32_t width, uint32_t height, const void
 
 /* `passes` successive passes; bit-identical to `passes` htc_render calls (each pixel's
  * samples run in order and keep its RNG stream). For the built-in recipes this is
- * htc_render_wavefront, so the program keeps the queues that form allocates. stats (optional, device uint64[HTC_STAT_COUNT])
+ * htc_render_wavefront, so the program keeps the queues that form allocates -- except for
+ * canvases under 2^19 pixels whose scene is Euclidean or holds fewer than 100 objects, which
+ * run the one-pass kernel once per pass (faster there; the same bits either way). stats (optional, device uint64[HTC_STAT_COUNT])
  * accumulates the HTC_STAT_* counters. */
 int htc_render_passes(htc_program *program, uint32_t width, uint32_t height, const void *scene,
                       size_t scene_size, float *canvas, uint32_t *seeds, uint32_t passes,
