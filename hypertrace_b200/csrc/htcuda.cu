@@ -3,15 +3,22 @@
 // Kernels:
 //   render_plain<R>      one thread per pixel, one pass: the reference's `render` kernel
 //                        (kernel/ocl/render/render.cl:6-27) launched over a (W,H) grid.
-//   render_persistent<R> one launch for P passes: warps pull pixels from a queue with
-//                        warp-aggregated atomics (ballot + popc), each lane runs its pixel's
-//                        P samples in order (the per-pixel RNG stream is sequential), and a
-//                        finished path is regenerated in place, so the object scan runs
-//                        with full warps instead of draining lanes as paths end.
+//   render_wave<R, FH>   one launch per hop depth of a pass (FH: hop 0 from the pixels, or a
+//                        later hop from a queue of ray states); survivors are appended to
+//                        the other queue with warp-aggregated atomics, so warps scan with
+//                        full lanes. The form htc_render_passes uses.
+//   render_batch_wave<RF, FH>  the same over many views at once, one launch per pass index,
+//                        hop depth and recipe, tiles of the views' queues cut on the device.
+//   render_persistent<R> one launch for P passes: warps pull pixels from a queue, each lane
+//                        runs its pixel's P samples in order and regenerates a finished path
+//                        in place (the allocation-free entry point uses it).
+//   render_batch         the persistent form over many views (HT_BATCH_MODE=1 builds).
 //   post kernels         extract / gamma / pack (processing/src/canvas.rs:126-135,176-186,
 //                        processing/src/filter/gamma.rs:10-19) and their fused form.
-// Both render kernels stage the scene's inverse object maps and shape indices in shared
-// memory once per block; the object scan reads them as warp-uniform broadcasts.
+// Every render kernel stages the scene's inverse object maps, distance-bound records and
+// shape indices in shared memory once per block (per view change in the batched kernels);
+// the object scan reads them as warp-uniform broadcasts. Each pixel's samples take the same
+// float operations in the same order in every form, so all forms give the same bits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
