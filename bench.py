@@ -42,6 +42,11 @@ FLOPS_PER_ESTIMATE = 30         # upper estimate of the nearest crossing, per ob
 ESTIMATE_OBJECTS = 32           # objects the estimate looks at (the first chunk)
 # The reference's own count (two ray maps of 256 ops per candidate: object/mapped.inl:32,34).
 REF_FLOPS_PER_OBJECT_TEST = 527
+# DRAM bytes per path advanced by one render_wave launch: dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of the hop-depth-1 launch of this frame (156.3 MB +
+# 93.1 MB for 2,073,600 paths; profiles/render_wave_hy1080p_200obj.md): the 68-byte ray state
+# read, the survivors' 68 bytes written, canvas and seed of the paths that end.
+DRAM_BYTES_PER_HOP = (156.262144e6 + 93.144064e6) / 2073600
 
 
 def parse_args():
@@ -386,7 +391,10 @@ def main():
             "hops_per_sample": hops / max(samples, 1),
             "exact_tests_per_hop": exact / max(hops, 1),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak_tflops if fp32_peak_tflops else None, "traffic": None,
+                         "frac": achieved / fp32_peak_tflops if fp32_peak_tflops else None,
+                         "traffic": DRAM_BYTES_PER_HOP * hops / launches,
+                         "traffic_source": "bytes per launch: the ncu capture's DRAM bytes per path of the "
+                                           "hop-1 launch x this run's paths per launch (hops / launches)",
                          "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",
                          "flops_per_launch": exec_flops / launches,
                          "reference_count_tflops": ref_flops / launches / per_launch_s / 1e12},
