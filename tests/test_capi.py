@@ -51,3 +51,15 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.lib()
+
+
+def test_newer_entry_points_reject_bad_arguments_without_device(built):
+    """The wavefront, batch-reservation and seed-fill entry points check their arguments
+    before touching a device."""
+    lib = _lib.lib()
+    assert lib.htc_render_wavefront(None, 4, 4, None, 0, None, None, 1, None, None) == _lib.HTC_ERR_INVALID
+    assert lib.htc_render_passes(None, 4, 4, None, 0, None, None, 1, None, None) == _lib.HTC_ERR_INVALID
+    assert lib.htc_batch_reserve(None, 1024, 8, None) == _lib.HTC_ERR_INVALID
+    assert b"batch" in lib.htc_last_error()
+    assert lib.htc_fill_seeds(None, 5, 0, 0, None) == _lib.HTC_ERR_INVALID
+    assert lib.htc_fill_seeds(None, 0, 0, 0, None) == _lib.HTC_OK   # nothing to fill
