@@ -57,8 +57,9 @@ def parse_args():
     ap.add_argument("--passes", type=int, default=4, help="passes (samples per pixel) per step")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["hy1080", "batched", "serving", "accuracy", "examples"], default="hy1080",
-                    help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views in one "
-                         "launch per step; serving: Poisson requests through the continuous-batching server")
+                    help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views, one launch "
+                         "per pass, hop depth and recipe over all of them; serving: Poisson requests through "
+                         "the continuous-batching server")
     ap.add_argument("--spp-scale", type=float, default=0.25, help="batched: scale of every view's spp")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
     ap.add_argument("--rates", type=str, default="50,200,1000,2000", help="serving: arrival rates (req/s)")

@@ -1,11 +1,12 @@
-"""Batched rendering: many views (either recipe, any resolution / hops / spp) per launch.
+"""Batched rendering: many views (either recipe, any resolution / hops / spp) per launch --
+one launch per pass index, hop depth and recipe, each over every view's queue of ray states.
 
 `BatchRenderer` wraps the `htc_batch_*` C ABI (include/htcuda.h). `config3()` builds the
 mixed workload: 96 views with resolutions from {256x256, 640x480, 1280x720, 1920x1080},
 spp uniform in {16, 32, ..., 256}, half Euclidean (8 unit spheres + ground plane, H = 4),
 half hyperbolic (20-200 objects, 60 % horospheres, translation distance <= 6, H = 8), each
-with a random camera. `autotune()` picks the tile size and residency by timing one launch per
-candidate on the actual views.
+with a random camera. `autotune()` picks the largest tile size and the residency by timing
+one render of one pass per candidate on the actual views.
 """
 from __future__ import annotations
 
@@ -58,7 +59,8 @@ class View:
 
 
 class BatchRenderer:
-    """htc_batch: a device tile table over a set of views, rendered by one persistent launch."""
+    """htc_batch: a set of views with their regions of the batch's wavefront queues; render()
+    runs every view's passes (bit-identical to rendering each view alone)."""
 
     def __init__(self, ctx: Context, max_views: int = 1024, max_tiles: int = 1 << 20):
         self.ctx = ctx
