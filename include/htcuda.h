@@ -177,7 +177,7 @@ typedef struct htc_view {
     uint32_t light_hops;
     uint32_t flags;          /* HTC_FLAG_* */
     int32_t address_width;   /* 32 or 64 */
-    uint32_t passes;         /* passes of this view rendered by each launch (0 = skip) */
+    uint32_t passes;         /* passes of this view each htc_batch_render renders (0 = skip) */
     uint32_t reserved;
 } htc_view;
 
