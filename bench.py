@@ -33,7 +33,7 @@ METRIC = "Msamples/s at 1080p hyperbolic (1920x1080, 200 objects, H=8)"
 UNIT = "Msamples/s"
 
 # Executed FP32 operations per unit of work in the CUDA path (static tally of the source,
-# each add/sub/mul/div/sqrt/log/sin/cos = 1): see DESIGN.md "Roofline".
+# each add/sub/mul/div/sqrt/log/sin/cos = 1).
 FLOPS_PER_EXACT_TEST = 219      # one inverse ray map (204) + shape distance test lower bound (15)
 FLOPS_PER_BOUND_TEST = 12       # world-space point bound of one object (hops x objects of them)
 FLOPS_PER_HIT_HOP = 936         # winner recompute + map back + interact maps + material
@@ -441,7 +441,7 @@ def bench_batched(args):
     for v in views:
         v.allocate(ctx)
     total_samples = sum(v.width * v.height * v.spp for v in views)
-    br = B.BatchRenderer(ctx, max_views=128, max_tiles=1 << 20)
+    br = B.BatchRenderer(ctx, max_views=128)
     tile, res, timings = B.autotune(br, views)
     stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
     dev_ms, steps, launches = 0.0, 0, 0

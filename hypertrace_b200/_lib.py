@@ -17,8 +17,6 @@ HTC_ERR_INVALID = -1
 HTC_ERR_CUDA = -2
 HTC_ERR_SCENE = -3
 HTC_ERR_UNSUPPORTED = -4
-HTC_ERR_BUDGET = -5
-HTC_ERR_TIMEOUT = -6
 
 HTC_RECIPE_HY = 1
 HTC_RECIPE_EU = 2
@@ -62,13 +60,12 @@ SIGNATURES = [
     ("htc_extract_gamma_pack", _i, [_u32, _u32, _u32, _f, _vp, _vp, _vp]),
     ("htc_fill_seeds", _i, [_vp, _u32, _u32, _u32, _vp]),
     ("htc_fp32_probe", _i, [_vp, _u32, _i, ctypes.POINTER(ctypes.c_double), _vp]),
-    ("htc_batch_create", _i, [_u32, _u32, ctypes.POINTER(_vp)]),
+    ("htc_batch_create", _i, [_u32, ctypes.POINTER(_vp)]),
     ("htc_batch_destroy", None, [_vp]),
     ("htc_batch_set_views", _i, [_vp, _vp, _u32, _u32, _u32, _vp]),
     ("htc_batch_render", _i, [_vp, _vp, _vp]),
     ("htc_batch_graph_launch", _i, [_vp, _vp, _vp]),
     ("htc_batch_check", _i, [_vp, _vp]),
-    ("htc_batch_tile_count", _i, [_vp, ctypes.POINTER(_u32)]),
     ("htc_batch_reserve", _i, [_vp, ctypes.c_uint64, _u32, _vp]),
 ]
 

@@ -62,10 +62,10 @@ class BatchRenderer:
     """htc_batch: a set of views with their regions of the batch's wavefront queues; render()
     runs every view's passes (bit-identical to rendering each view alone)."""
 
-    def __init__(self, ctx: Context, max_views: int = 1024, max_tiles: int = 1 << 20):
+    def __init__(self, ctx: Context, max_views: int = 1024):
         self.ctx = ctx
         h = ctypes.c_void_p()
-        _lib.call("htc_batch_create", max_views, max_tiles, ctypes.byref(h))
+        _lib.call("htc_batch_create", max_views, ctypes.byref(h))
         self.handle = h
         self.tile_pixels = 2048
         self.blocks_per_sm = 0
@@ -102,10 +102,6 @@ class BatchRenderer:
         """Size the wavefront queues for view sets of up to `pixels` pixels and `max_hops` hops."""
         _lib.call("htc_batch_reserve", self.handle, pixels, max_hops, self.ctx.stream())
 
-    def tile_count(self) -> int:
-        n = ctypes.c_uint32()
-        _lib.call("htc_batch_tile_count", self.handle, ctypes.byref(n))
-        return n.value
 
 
 def random_hom3(rng: np.random.Generator) -> S.Hom3:

@@ -12,7 +12,6 @@
 //   render_persistent<R> one launch for P passes: warps pull pixels from a queue, each lane
 //                        runs its pixel's P samples in order and regenerates a finished path
 //                        in place (the allocation-free entry point uses it).
-//   render_batch         the persistent form over many views (HT_BATCH_MODE=1 builds).
 //   post kernels         extract / gamma / pack (processing/src/canvas.rs:126-135,176-186,
 //                        processing/src/filter/gamma.rs:10-19) and their fused form.
 // Every render kernel stages the scene's inverse object maps, distance-bound records and
@@ -55,10 +54,6 @@ thread_local std::string g_last_error;
 // persistent kernel 208.6.
 #ifndef HT_PASSES_MODE
 #define HT_PASSES_MODE 2
-#endif
-// htc_batch_render: 2 = wavefronts (render_batch_wave), 1 = one persistent launch (render_batch).
-#ifndef HT_BATCH_MODE
-#define HT_BATCH_MODE 2
 #endif
 // Batched wavefronts: 1 = one launch per recipe for each (pass, hop depth), 0 = one launch for both.
 #ifndef HT_BATCH_SPLIT
@@ -299,7 +294,7 @@ __device__ __forceinline__ void flush_lane_stats(uint64_t *stats, const LaneStat
     }
 }
 
-// The persistent lane loop shared by render_persistent and render_batch: warps take pixel
+// The persistent lane loop of render_persistent: warps take pixel
 // indices [first, first + count) from `*counter` (global or shared memory) with one atomic
 // per warp; each lane renders its pixel's `passes` samples in order and regenerates a camera
 // ray as soon as a path ends. Returns when the warp has no pixel left.
@@ -551,12 +546,6 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
 }
 
 // ============================================================================ batch
-// Many views (scenes, resolutions, pass counts, either recipe) in one persistent launch.
-// Blocks take tiles (view, pixel range) from a global queue; a block stages a view's scene
-// in shared memory only when its tile's view differs from the one it holds; the block's
-// warps then pull the tile's pixels from a shared-memory counter. Per-pixel sample order is
-// the same as in render_persistent, so every view's result is bit-identical to rendering it
-// alone.
 struct BatchView {          // device copy of htc_view plus host-derived fields
     const uint8_t *scene;
     uint64_t scene_size;
@@ -570,78 +559,6 @@ struct BatchView {          // device copy of htc_view plus host-derived fields
     uint32_t max_objects;   // objects the scene buffer can hold
     uint64_t qoff;          // first slot of the view's region in the wavefront queues
 };
-struct BatchTile { uint32_t view, first, count; };
-
-__global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_batch(
-    const BatchView *__restrict__ views, const BatchTile *__restrict__ tiles, uint32_t n_tiles,
-    uint32_t smem_objects, uint64_t *stats, uint32_t *err, uint32_t *queue) {
-    extern __shared__ float4 smem[];
-    __shared__ uint32_t s_hdr[2];
-    __shared__ uint32_t s_tile, s_next;
-    __shared__ int s_staged_view, s_staged_ok;
-    const SceneSmem sm = carve_scene(smem, smem_objects);
-    StagedScene s;
-    s.n = 0;
-    LaneStats st;
-    uint64_t object_tests = 0;
-    if (threadIdx.x == 0) s_staged_view = -1;
-    for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            s_tile = atomicAdd(&queue[0], 1u);
-            s_next = 0;
-        }
-        __syncthreads();
-        const uint32_t t = s_tile;
-        if (t >= n_tiles) break;
-        const BatchTile tile = tiles[t];
-        const BatchView &v = views[tile.view];
-        const int32_t recipe = v.recipe;
-        if ((int)tile.view != s_staged_view) {
-            bool ok;
-            if (recipe == RECIPE_HY)
-                ok = stage_scene<RECIPE_HY>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, sm, s_hdr);
-            else
-                ok = stage_scene<RECIPE_EU>(v.scene, v.scene_size, min(v.max_objects, smem_objects), v.address_width,
-                                            err, s, sm, s_hdr);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                s_staged_view = (int)tile.view;
-                s_staged_ok = ok ? 1 : 0;
-            }
-            __syncthreads();
-        }
-        // (every thread staged the current view, so its StagedScene `s` still describes it)
-        if (!s_staged_ok) continue;
-        const uint32_t hops_before = st.hops;
-        if (recipe == RECIPE_HY)
-            trace_pixels<RECIPE_HY>(s, &s_next, tile.first, tile.count, v.width, v.height, v.hops, v.passes, v.flags,
-                                    v.canvas, v.seeds, st);
-        else
-            trace_pixels<RECIPE_EU>(s, &s_next, tile.first, tile.count, v.width, v.height, v.hops, v.passes, v.flags,
-                                    v.canvas, v.seeds, st);
-        object_tests += (uint64_t)(st.hops - hops_before) * s.n;
-    }
-    if (stats) {
-        uint64_t samples = st.samples, hops = st.hops, hits = st.hits, exact = st.exact, tests = object_tests;
-        for (int off = 16; off > 0; off >>= 1) {
-            samples += __shfl_down_sync(0xffffffffu, samples, off);
-            hops += __shfl_down_sync(0xffffffffu, hops, off);
-            hits += __shfl_down_sync(0xffffffffu, hits, off);
-            exact += __shfl_down_sync(0xffffffffu, exact, off);
-            tests += __shfl_down_sync(0xffffffffu, tests, off);
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd((unsigned long long *)&stats[HTC_STAT_SAMPLES], (unsigned long long)samples);
-            atomicAdd((unsigned long long *)&stats[HTC_STAT_HOPS], (unsigned long long)hops);
-            atomicAdd((unsigned long long *)&stats[HTC_STAT_OBJECT_TESTS], (unsigned long long)tests);
-            atomicAdd((unsigned long long *)&stats[HTC_STAT_HITS], (unsigned long long)hits);
-            atomicAdd((unsigned long long *)&stats[HTC_STAT_EXACT_TESTS], (unsigned long long)exact);
-        }
-    }
-    rewind_queue(queue);
-}
 
 // Wavefront form of the batch: one launch per (pass, hop depth) over every view. Each view
 // has its own region of the two queues and its own append counter; the launch cuts the
@@ -1267,12 +1184,9 @@ int htc_fill_seeds(uint32_t *seeds, uint32_t n, uint32_t global_seed, uint32_t o
 }  // extern "C"
 
 struct htc_batch {
-    uint32_t max_views, max_tiles;
+    uint32_t max_views;
     BatchView *d_views;
-    BatchTile *d_tiles;
-    uint32_t *d_queue;   // [0] next tile, [1] finished blocks
     uint32_t *d_err;
-    uint32_t n_tiles;
     uint32_t smem_objects;
     uint32_t blocks_per_sm;
     uint32_t tile_pixels;
@@ -1280,12 +1194,9 @@ struct htc_batch {
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
     std::vector<BatchView> h_views;
-    std::vector<BatchTile> h_tiles;
     // Two pinned staging slots for the asynchronous descriptor upload; slot i may be
     // rewritten once its last copy (event staged[i]) has run.
     BatchView *p_views[2];
-    BatchTile *p_tiles[2];
-    size_t p_tiles_cap[2];
     cudaEvent_t staged[2];
     int slot;
     // wavefront form: view order (expensive first), queues, counters
@@ -1306,7 +1217,6 @@ static void batch_free(htc_batch *b) {
             cudaEventDestroy(b->staged[i]);
         }
         if (b->p_views[i]) cudaFreeHost(b->p_views[i]);
-        if (b->p_tiles[i]) cudaFreeHost(b->p_tiles[i]);
         if (b->p_order[i]) cudaFreeHost(b->p_order[i]);
     }
     if (b->d_order) cudaFree(b->d_order);
@@ -1315,8 +1225,6 @@ static void batch_free(htc_batch *b) {
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_views);
-    cudaFree(b->d_tiles);
-    cudaFree(b->d_queue);
     cudaFree(b->d_err);
     delete b;
 }
@@ -1384,42 +1292,21 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
     return HTC_OK;
 }
 
-static int batch_launch(htc_batch *b, uint64_t *stats, cudaStream_t st) {
-    if (HT_BATCH_MODE == 2) return batch_launch_wave(b, stats, st);
-    if (b->n_tiles == 0) return HTC_OK;
-    const size_t smem = smem_bytes(b->smem_objects);
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_batch, 128, smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)per_sm * (uint64_t)b->num_sms;
-    if (blocks > b->n_tiles) blocks = b->n_tiles;
-    render_batch<<<(unsigned)blocks, 128, smem, st>>>(b->d_views, b->d_tiles, b->n_tiles, b->smem_objects, stats,
-                                                      b->d_err, b->d_queue);
-    HTC_CUDA(cudaGetLastError());
-    return HTC_OK;
-}
-
 extern "C" {
 
-int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
+int htc_batch_create(uint32_t max_views, htc_batch **out) {
     if (!out) return fail(HTC_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    if (max_views == 0 || max_tiles == 0) return fail(HTC_ERR_INVALID, "max_views and max_tiles must be positive");
+    if (max_views == 0) return fail(HTC_ERR_INVALID, "max_views must be positive");
     int dev = 0;
     HTC_CUDA(cudaGetDevice(&dev));
     htc_batch *b = new htc_batch();
     b->max_views = max_views;
-    b->max_tiles = max_tiles;
     cudaError_t e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_views, sizeof(BatchView) * max_views);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * max_tiles);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_order, 2 * sizeof(uint32_t) * max_views);   // all, then by recipe
     if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
         e = cudaHostAlloc(reinterpret_cast<void **>(&b->p_views[i]), sizeof(BatchView) * max_views, cudaHostAllocDefault);
@@ -1428,9 +1315,7 @@ int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out) {
     }
     if (e == cudaSuccess) {
         b->max_smem -= 1024;
-        e = cudaFuncSetAttribute(render_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem);
-        if (e == cudaSuccess)
-            e = batch_wave_smem_attr<0>(b->max_smem);
+        e = batch_wave_smem_attr<0>(b->max_smem);
         if (e == cudaSuccess) e = batch_wave_smem_attr<RECIPE_HY>(b->max_smem);
         if (e == cudaSuccess) e = batch_wave_smem_attr<RECIPE_EU>(b->max_smem);
     }
@@ -1486,7 +1371,6 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     if (n_views && !views) return fail(HTC_ERR_INVALID, "views is NULL");
     if (tile_pixels == 0) return fail(HTC_ERR_INVALID, "tile_pixels must be positive");
     b->h_views.assign(n_views, BatchView());
-    b->h_tiles.clear();
     uint32_t smem_objects = 0;
     std::vector<std::pair<double, uint32_t>> order;
     for (uint32_t i = 0; i < n_views; ++i) {
@@ -1533,21 +1417,11 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
         hops_max = std::max(hops_max, d.hops);
         passes_max = std::max(passes_max, d.passes);
     }
-    for (const auto &o : order) {   // tiles of the persistent batch kernel only
-        if (HT_BATCH_MODE != 1) break;
-        const BatchView &d = b->h_views[o.second];
-        const uint32_t total = d.width * d.height;
-        for (uint32_t first = 0; first < total; first += tile_pixels) {
-            if (b->h_tiles.size() >= b->max_tiles) return fail(HTC_ERR_INVALID, "more tiles than the batch was created for (raise max_tiles or tile_pixels)");
-            b->h_tiles.push_back({o.second, first, std::min(tile_pixels, total - first)});
-        }
-    }
-    b->n_tiles = (uint32_t)b->h_tiles.size();
     b->smem_objects = smem_objects;
     b->blocks_per_sm = blocks_per_sm;
     b->tile_pixels = tile_pixels;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    if (HT_BATCH_MODE == 2) {
+    {
         int rc = batch_grow(b, slots, (size_t)(n_views + 3) * hops_max, st);
         if (rc) return rc;
     }
@@ -1560,13 +1434,6 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     const int k = b->slot;
     b->slot ^= 1;
     HTC_CUDA(cudaEventSynchronize(b->staged[k]));
-    if (b->n_tiles > b->p_tiles_cap[k]) {
-        if (b->p_tiles[k]) HTC_CUDA(cudaFreeHost(b->p_tiles[k]));
-        b->p_tiles[k] = nullptr;
-        const size_t cap = std::max<size_t>(b->n_tiles, 4096);
-        HTC_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&b->p_tiles[k]), sizeof(BatchTile) * cap, cudaHostAllocDefault));
-        b->p_tiles_cap[k] = cap;
-    }
     if (n_views) std::memcpy(b->p_views[k], b->h_views.data(), sizeof(BatchView) * n_views);
     // the cost order of every view, then the same order split by recipe
     uint32_t *po = b->p_order[k];
@@ -1577,9 +1444,7 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     for (uint32_t i = 0; i < b->n_order; ++i)
         if (b->h_views[order[i].second].recipe != RECIPE_HY) po[b->n_order + b->n_hy + b->n_eu++] = order[i].second;
     if (b->n_order) HTC_CUDA(cudaMemcpyAsync(b->d_order, po, 2 * sizeof(uint32_t) * b->n_order, cudaMemcpyHostToDevice, st));
-    if (b->n_tiles) std::memcpy(b->p_tiles[k], b->h_tiles.data(), sizeof(BatchTile) * b->n_tiles);
     if (n_views) HTC_CUDA(cudaMemcpyAsync(b->d_views, b->p_views[k], sizeof(BatchView) * n_views, cudaMemcpyHostToDevice, st));
-    if (b->n_tiles) HTC_CUDA(cudaMemcpyAsync(b->d_tiles, b->p_tiles[k], sizeof(BatchTile) * b->n_tiles, cudaMemcpyHostToDevice, st));
     HTC_CUDA(cudaEventRecord(b->staged[k], st));
     if (b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
@@ -1588,7 +1453,7 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
 
 int htc_batch_render(htc_batch *b, uint64_t *stats, void *stream) {
     if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
-    return batch_launch(b, stats, reinterpret_cast<cudaStream_t>(stream));
+    return batch_launch_wave(b, stats, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int htc_batch_graph_launch(htc_batch *b, uint64_t *stats, void *stream) {
@@ -1599,7 +1464,7 @@ int htc_batch_graph_launch(htc_batch *b, uint64_t *stats, void *stream) {
         HTC_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         int rc = HTC_OK;
-        if (e == cudaSuccess) rc = batch_launch(b, stats, cap);
+        if (e == cudaSuccess) rc = batch_launch_wave(b, stats, cap);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);
@@ -1628,18 +1493,15 @@ int htc_batch_check(htc_batch *b, void *stream) {
     return HTC_OK;
 }
 
-int htc_batch_tile_count(const htc_batch *b, uint32_t *n_tiles) {
-    if (!b || !n_tiles) return fail(HTC_ERR_INVALID, "batch or n_tiles is NULL");
-    *n_tiles = b->n_tiles;
-    return HTC_OK;
-}
 
 // ---------------------------------------------------------------- allocation-free entry
 // Scratch of htc_render_passes_noalloc: the persistent kernel's work-queue words
-// ([0] next pixel, [1] finished blocks) and a fallback error word ([2]). A file-scope
-// device array, so the entry point never allocates; it lives on every device that loads
-// this library until the process exits. In host code `g_noalloc_scratch` is only a
-// stand-in for the symbol: its device address comes from cudaGetSymbolAddress.
+// ([0] next pixel, [1] finished blocks) and the error word the kernel writes when the caller
+// passes no `status` ([2]; nothing reads it, so such a caller gets no error report, as the
+// header says). A file-scope device array, so the entry point never allocates; it lives on
+// every device that loads this library until the process exits. In host code
+// `g_noalloc_scratch` is only a stand-in for the symbol: its device address comes from
+// cudaGetSymbolAddress.
 constexpr uint32_t NOALLOC_SCRATCH_WORDS = 64;   // 256 bytes
 constexpr uint64_t NOALLOC_MAX_PIXELS = 1ull << 31;   // the queue word counts pixels
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
@@ -1652,7 +1514,8 @@ int g_noalloc_sms[NOALLOC_MAX_DEVICES];
 int g_noalloc_smem[NOALLOC_MAX_DEVICES];
 
 // Once per device, with that device current: resolve the scratch address and the launch
-// limits. Allocates nothing.
+// limits. Allocates nothing. The cached address and kernel attributes outlive a device reset,
+// which the header therefore excludes after the first call.
 int noalloc_setup(int dev, uint32_t **scratch, int *num_sms, int *max_smem) {
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(HTC_ERR_UNSUPPORTED, "device index beyond the supported range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);

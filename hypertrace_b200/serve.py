@@ -97,7 +97,7 @@ class Server:
         self.ctx = ctx
         self.budget = hbm_budget_bytes
         self.step_samples = step_samples    # work of one step: bounds the wait of a new arrival
-        self.renderer = BatchRenderer(ctx, max_views=4096, max_tiles=1 << 21)
+        self.renderer = BatchRenderer(ctx, max_views=4096)
         # queues for the largest step (its views cover at most step_samples pixels, plus one
         # oversized job), so that set_views never has to grow them mid-run
         self.renderer.reserve(min(step_samples + 1920 * 1080, hbm_budget_bytes // 136), 8)

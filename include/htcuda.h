@@ -25,8 +25,6 @@ extern "C" {
 #define HTC_ERR_CUDA (-2)         /* a CUDA runtime call failed */
 #define HTC_ERR_SCENE (-3)        /* scene bytes failed validation (device-side check) */
 #define HTC_ERR_UNSUPPORTED (-4)  /* configuration this build does not serve */
-#define HTC_ERR_BUDGET (-5)       /* admission refused: memory budget exceeded */
-#define HTC_ERR_TIMEOUT (-6)      /* a bounded device wait or work loop gave up */
 
 /* ---------------------------------------------------------------- scene recipes
  * The scene types the hand-written kernels serve (the Rust types that the reference's
@@ -98,7 +96,7 @@ int htc_program_build(const char *scene_type, uint32_t light_hops, int address_w
  * objects: the bytes up to the first element); a smaller scene buffer is rejected. */
 int htc_program_static_size(const htc_program *program, uint64_t *bytes);
 /* Reads and clears the device-side error word of the program's last launches
- * (synchronises `stream`). Returns HTC_OK or HTC_ERR_SCENE / HTC_ERR_TIMEOUT. */
+ * (synchronises `stream`). Returns HTC_OK or HTC_ERR_SCENE. */
 int htc_program_check(htc_program *program, void *stream);
 
 /* ---------------------------------------------------------------- buffers */
@@ -147,11 +145,15 @@ int htc_render_wavefront(htc_program *program, uint32_t width, uint32_t height, 
  * flags are passed directly; the work-queue words live in a 256-byte file-scope device array
  * that every device loading the library holds until exit. The first call on a device
  * resolves that array's address (cudaGetSymbolAddress) and the launch limits, so make the
- * first call on each device before any stream capture. Calls share the array and zero it
- * on entry: calls that overlap on the GPU race and must not be issued concurrently.
- * Limit: width*height <= 2^31 pixels (HTC_ERR_UNSUPPORTED beyond). `status` (optional,
- * device uint32, zeroed by the caller) receives the scene-validation error bits that
- * htc_program_check would report (non-zero = HTC_ERR_SCENE). */
+ * first call on each device before any stream capture; they are kept for the rest of the
+ * process, so resetting the device (cudaDeviceReset) after that first call is not supported.
+ * Calls share the array and zero its queue words on entry: calls that overlap on the GPU
+ * race and must not be issued concurrently.
+ * Limit: width*height <= 2^31 pixels (HTC_ERR_UNSUPPORTED beyond). `status` (device uint32,
+ * zeroed by the caller) receives the scene-validation error bits that htc_program_check
+ * would report (non-zero = HTC_ERR_SCENE); a scene that fails validation is not rendered
+ * (canvas and seeds keep their contents). `status` may be NULL, but then such a failure is
+ * reported nowhere: pass it wherever the scene bytes are not known to be valid. */
 int htc_render_passes_noalloc(int recipe, uint32_t light_hops, int address_width, uint32_t flags,
                               uint32_t width, uint32_t height, const void *scene, size_t scene_size,
                               float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats,
@@ -163,10 +165,11 @@ int htc_render_ex(htc_program *program, uint32_t width, uint32_t height, const v
                   void *stream);
 
 /* ---------------------------------------------------------------- batches
- * Many views -- scenes of either recipe, resolutions, hop counts and pass counts -- in one
- * persistent launch (no counterpart in the reference, whose Pipeline renders one view per
- * enqueue). Each view's result is bit-identical to rendering it alone with
- * htc_render_passes: pixels keep their own RNG streams and sample order. */
+ * Many views -- scenes of either recipe, resolutions, hop counts and pass counts -- rendered
+ * together: one launch per pass index, hop depth and recipe covers every view's queue of ray
+ * states (no counterpart in the reference, whose Pipeline renders one view per enqueue).
+ * Each view's result is bit-identical to rendering it alone with htc_render_passes: pixels
+ * keep their own RNG streams and sample order. */
 typedef struct htc_view {
     const void *scene;       /* device pointer to the serialized scene bytes */
     uint64_t scene_size;
@@ -182,10 +185,12 @@ typedef struct htc_view {
 } htc_view;
 
 typedef struct htc_batch htc_batch;
-int htc_batch_create(uint32_t max_views, uint32_t max_tiles, htc_batch **out);
+int htc_batch_create(uint32_t max_views, htc_batch **out);
 void htc_batch_destroy(htc_batch *batch);
-/* Uploads the views and cuts them into tiles of `tile_pixels` pixels (most expensive views
- * first); blocks_per_sm caps residency (0 = as many as fit). Asynchronous on `stream`
+/* Uploads the views (most expensive first, each given a region of the batch's queues);
+ * `tile_pixels` caps the queue slots a block takes at a time (each launch cuts its tiles on
+ * the device, shorter when its paths are few); blocks_per_sm caps residency (0 = as many as
+ * fit). Asynchronous on `stream`
  * (double-buffered pinned staging): the next launch on `stream` sees the new views, launches
  * already enqueued keep theirs. Blocks only while the staging slot it reuses is still being
  * copied (two calls back). */
@@ -203,9 +208,6 @@ int htc_batch_render(htc_batch *batch, uint64_t *stats, void *stream);
 int htc_batch_graph_launch(htc_batch *batch, uint64_t *stats, void *stream);
 /* Reads and clears the batch's device error word (synchronises `stream`). */
 int htc_batch_check(htc_batch *batch, void *stream);
-/* Tiles the last htc_batch_set_views cut for a persistent launch; the wavefront form (the
- * default) cuts its tiles on the device at every launch and reports 0. */
-int htc_batch_tile_count(const htc_batch *batch, uint32_t *n_tiles);
 
 /* ---------------------------------------------------------------- post chain
  * Extractor (processing/src/canvas.rs:126-135): image = canvas / passes.

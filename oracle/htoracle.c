@@ -631,6 +631,15 @@ void HTO(extract_gamma_pack)(uint32_t n_pixels, uint32_t passes, float gamma, co
     }
 }
 
+/* Pack alone (canvas.rs:176-186): u8 = convert_uchar4(0xFF * clamp(x, 0, 1)). OpenCL's
+ * clamp is fmin(fmax(x, 0), 1), so NaN gives 0; the default conversion rounds toward zero. */
+void HTO(pack)(uint32_t n_pixels, const float *image, uint8_t *packed) {
+    for (uint32_t i = 0; i < 4u * n_pixels; ++i) {
+        float c = fminf(fmaxf(image[i], 0.0f), 1.0f);
+        packed[i] = (uint8_t)(255.0f * c);
+    }
+}
+
 int HTO(real_size)(void) { return (int)sizeof(R); }
 
 void HTO(rng_uniforms)(uint32_t seed, uint32_t n, double *out, uint32_t *state_out) {

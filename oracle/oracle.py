@@ -27,10 +27,11 @@ _libs = {}
 
 
 def build(reference_root: Optional[str] = None) -> None:
-    """Compile the restatement (always) and oracle/_ref (when the reference tree exists)."""
+    """Compile the restatement (always) and oracle/_ref from the reference tree at
+    `reference_root` (or $HT_REFERENCE_ROOT) when one is given and present."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref = reference_root or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "kernel", "ocl")):
+    ref = reference_root or os.environ.get("HT_REFERENCE_ROOT")
+    if ref and os.path.isdir(os.path.join(ref, "kernel", "ocl")):
         subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={ref}"], check=True)
 
 
@@ -120,6 +121,18 @@ def extract_gamma_pack(canvas: np.ndarray, passes: int, gamma: float):
     packed = np.zeros(cv.shape, dtype=np.uint8)
     fn(cv.shape[0], passes, gamma, _ptr(cv, _f32p), _ptr(img, _f32p), _ptr(packed, _u8p))
     return img, packed
+
+
+def pack(image: np.ndarray) -> np.ndarray:
+    """Pack alone on the CPU (canvas.rs:176-186): float image -> RGBA8, toward zero."""
+    lib = _load(os.path.join(HERE, "libhtoracle_f32.so"))
+    fn = lib.hto32_pack
+    fn.restype = None
+    fn.argtypes = [ctypes.c_uint32, _f32p, _u8p]
+    img = np.ascontiguousarray(image, dtype=np.float32).reshape(-1, 4)
+    packed = np.zeros(img.shape, dtype=np.uint8)
+    fn(img.shape[0], _ptr(img, _f32p), _ptr(packed, _u8p))
+    return packed
 
 
 def rng_uniforms(seed: int, n: int, impl: str = "port", precision: int = 32):

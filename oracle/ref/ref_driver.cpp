@@ -519,7 +519,7 @@ inline __global const ConstBg *ht_eu_scene__background__gc(__global const HtEuSc
 
 // ============================================================================ parsing
 // Serialized layout (AddressWidth X32 or X64, double_support=false), little-endian.
-// Offsets are derived in DESIGN.md ("Scene byte ABI"); they follow
+// Offsets (derived in hypertrace_b200/scene.py) follow
 // type-macros/src/entity.rs:7-186 (align = lcm of fields, fields aligned, size rounded
 // to align) with float3 padded to 16 bytes (types/src/primitive/vector.rs:95-106).
 

@@ -33,7 +33,7 @@ def test_batch_equals_alone(built, graph, tile):
     for v in views + alone:
         v.allocate(ctx)
     passes = [1, 3, 2, 4, 1, 2]
-    br = B.BatchRenderer(ctx, max_views=16, max_tiles=4096)
+    br = B.BatchRenderer(ctx, max_views=16)
     br.set_views(views, passes, tile_pixels=tile, blocks_per_sm=0)
     for _ in range(2):
         br.render(graph=graph)
@@ -53,7 +53,7 @@ def test_batch_zero_pass_view_untouched(built):
     for v in views:
         v.allocate(ctx)
     before = views[1].canvas.image.clone()
-    br = B.BatchRenderer(ctx, max_views=4, max_tiles=1024)
+    br = B.BatchRenderer(ctx, max_views=4)
     br.set_views(views, [1, 0, 1], tile_pixels=256)
     br.render()
     br.check()
@@ -67,7 +67,7 @@ def test_batch_autotune_restores_state(built):
     for v in views:
         v.allocate(ctx)
     snap = [v.canvas.seeds.clone() for v in views]
-    br = B.BatchRenderer(ctx, max_views=16, max_tiles=4096)
+    br = B.BatchRenderer(ctx, max_views=16)
     tile, res, t = B.autotune(br, views, tiles=(128, 1024), residency=(4, 6))
     assert (tile, res) in t and len(t) == 4
     for v, s in zip(views, snap):
@@ -86,7 +86,7 @@ def test_batch_large_views_adaptive_tiles(built):
     views, alone = make(), make()
     for v in views + alone:
         v.allocate(ctx)
-    br = B.BatchRenderer(ctx, max_views=8, max_tiles=16)
+    br = B.BatchRenderer(ctx, max_views=8)
     br.reserve(2 * 1920 * 1080 + 96 * 40, 8)
     br.set_views(views, [2, 2, 2], tile_pixels=2048, blocks_per_sm=0)
     br.render()
@@ -111,7 +111,7 @@ def test_batch_mixed_hop_counts(built):
     views, alone = make(), make()
     for v in views + alone:
         v.allocate(ctx)
-    br = B.BatchRenderer(ctx, max_views=8, max_tiles=16)
+    br = B.BatchRenderer(ctx, max_views=8)
     br.set_views(views, [v.spp for v in views], tile_pixels=512)
     br.render(graph=True)
     br.check()
