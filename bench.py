@@ -12,6 +12,19 @@ one-pass kernel (one launch per pass) and the persistent kernel are timed beside
     python bench.py [--gpus N --steps K --warmup W --passes P]
     python bench.py --impl reference      # the reference's own kernel code on the host CPU
 
+On one GPU the line also carries, measured after the timed region:
+  parity    the full frame rendered for 16 passes against the reference's kernel code
+            (oracle/_ref) on random pixels: mismatched / bit-exact fractions, and the
+            per-pixel error against the FP64 build of the same code;
+  batched   the mixed workload of 96 views (resolutions 256x256 to 1920x1080, spp 16-256,
+            half Euclidean, half hyperbolic with 20-200 objects) through one launch per pass,
+            hop depth and recipe over all views, against the same views rendered one at a
+            time with the one-pass kernel (one launch per pass) and with wavefronts;
+  serving   Poisson arrivals at 50 and 2000 requests/s (70 % interactive 1280x720 8-spp
+            frames with a moving camera, 30 % batch jobs) through the continuous-batching
+            server, against a FIFO server that renders one request at a time with the
+            one-pass kernel: throughput and p50 / p99 latency per class.
+
 Under torchrun (N > 1) each rank renders its own frame (replicas: the path has no exchange
 step); the reported value is all ranks' samples over the slowest rank's device time.
 """
@@ -60,9 +73,12 @@ def parse_args():
                     help="hy1080: the headline 1080p hyperbolic frame; batched: 96 mixed views, one launch "
                          "per pass, hop depth and recipe over all of them; serving: Poisson requests through "
                          "the continuous-batching server")
-    ap.add_argument("--spp-scale", type=float, default=0.25, help="batched: scale of every view's spp")
-    ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
-    ap.add_argument("--rates", type=str, default="50,200,1000,2000", help="serving: arrival rates (req/s)")
+    ap.add_argument("--spp-scale", type=float, default=1.0, help="batched: scale of every view's spp")
+    ap.add_argument("--requests", type=int, default=1000, help="serving: requests per arrival rate")
+    ap.add_argument("--rates", type=str, default="50,2000", help="serving: arrival rates (req/s)")
+    ap.add_argument("--parity-pixels", type=int, default=4096, help="parity: pixels compared with the oracle")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the parity, batched and serving measurements of the default line")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -147,6 +163,57 @@ def cpu_baseline(wl, seconds: float, threads: int = 0):
     dt = time.perf_counter() - t0
     return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"{samples} samples (random pixels of the 1920x1080 frame, 1 pass each) in {dt:.1f} s"}
+
+
+def measure_parity(ctx, wl, n_pixels: int, passes: int = 16):
+    """Parity of the timed path at the workload's own size, outside the timed region: the
+    whole frame rendered for `passes` passes (wavefronts) from its seeds, `n_pixels` random
+    pixels compared with the reference's own kernel code built for the host (oracle/_ref,
+    f32) over the same passes; a pixel is mismatched when its RNG state differs or its
+    radiance is off by more than 1e-4 relative (floor 1e-3). The FP64 build of the same
+    code gives each pixel's error of the FP32 result (relative, floor 1e-3), over all
+    sampled pixels and over those whose path the FP64 run takes too (same RNG state)."""
+    import torch
+    from hypertrace_b200 import processing as P
+    from hypertrace_b200 import _lib
+    from oracle import oracle
+    sc = wl.scene
+    W, H = wl.width, wl.height
+    impl = "reference" if oracle.ref_available(32) and oracle.ref_available(64) else "port"
+    buf = P.EntityBuffer(ctx, sc)
+    canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
+    seeds0 = canvas.seeds.cpu().numpy().view(np.uint32).copy()
+    P.Render(ctx, sc.recipe, sc.hops, _lib.HTC_FLAG_JITTER_YX).render_passes(buf, canvas, passes)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(99)
+    pix = np.sort(rng.choice(W * H, n_pixels, replace=False)).astype(np.uint32)
+    gpu = canvas.image.cpu().numpy().reshape(-1, 4)[pix]
+    gseeds = canvas.seeds.cpu().numpy().view(np.uint32)[pix]
+    cores = os.cpu_count() or 1
+    data = sc.to_bytes()
+    t0 = time.perf_counter()
+    f32 = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds0[pix], passes=passes, impl=impl,
+                        threads=cores, flags=oracle.JITTER_YX)
+    f64 = oracle.render(data, sc.recipe, sc.hops, W, H, pix, seeds0[pix], passes=passes, impl=impl,
+                        threads=cores, flags=oracle.JITTER_YX, precision=64)
+    cpu_s = time.perf_counter() - t0
+    same = gseeds == f32.seeds
+    rel = (np.abs(gpu - f32.canvas) / np.maximum(np.abs(f32.canvas), 1e-3)).max(axis=1)
+    mismatch = (~same) | (rel > 1e-4)
+    exact = same & np.all(gpu.view(np.uint32) == f32.canvas.view(np.uint32), axis=1)
+    g = gpu[:, :3] / passes
+    c64 = f64.canvas[:, :3] / passes
+    rel64 = (np.abs(g - c64) / np.maximum(np.abs(c64), 1e-3)).max(axis=1)
+    same64 = f64.seeds == gseeds
+    return {"pixels": int(n_pixels), "passes": passes, "checker": f"oracle/_ref ({impl})", "cpu_s": round(cpu_s, 2),
+            "mismatch_frac": float(mismatch.mean()), "rng_mismatch_frac": float((~same).mean()),
+            "hops_per_pixel": f32.stats["hops"] / n_pixels,
+            "mismatch_per_hop": float(mismatch.mean()) / max(f32.stats["hops"] / n_pixels, 1e-9),
+            "bit_exact_frac": float(exact.mean()),
+            "f64_rel_err": {"median": float(np.median(rel64)), "mean": float(rel64.mean()), "max": float(rel64.max()),
+                            "same_path_frac": float(same64.mean()),
+                            "same_path_max": float(rel64[same64].max()) if same64.any() else None,
+                            "same_path_mean": float(rel64[same64].mean()) if same64.any() else None}}
 
 
 def run_reference(args, rank: int):
@@ -379,6 +446,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl, args.cpu_seconds)
 
+    # ---------------- untimed extras of the one-GPU line: parity at size, batched, serving
+    parity = batched = serving = None
+    if world == 1 and not args.no_extras:
+        parity = measure_parity(ctx, wl, args.parity_pixels)
+        batched = measure_batched(args)
+        serving = measure_serving(args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -399,6 +473,9 @@ def main():
                          "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",
                          "flops_per_launch": exec_flops / launches,
                          "reference_count_tflops": ref_flops / launches / per_launch_s / 1e12},
+            "parity": parity,
+            "batched": batched,
+            "serving": serving,
             "persistent": persistent,
             "plain_one_pass": plain,
             "e2e": e2e,
@@ -424,7 +501,7 @@ def _time_ms(fn, stream):
     return e0.elapsed_time(e1)
 
 
-def bench_batched(args):
+def measure_batched(args):
     """The mixed workload (96 views: resolutions from {256^2, 640x480, 1280x720, 1920x1080},
     spp in {16..256} x --spp-scale, half Euclidean / half hyperbolic with 20-200 objects):
     batched wavefronts (one launch per pass and hop depth covering every view, autotuned tile
@@ -490,17 +567,23 @@ def bench_batched(args):
 
     plain = per_view(False)
     single = per_view(True)
+    return {"workload": "mixed-96-views", "spp_scale": args.spp_scale, "total_samples": total_samples,
+            "passes_per_step": 16, "batched": batched, "plain_per_view": plain, "wavefront_per_view": single,
+            "speedup_vs_plain": batched["value"] / plain["value"],
+            "speedup_vs_wavefront_per_view": batched["value"] / single["value"]}
+
+
+def bench_batched(args):
+    out = measure_batched(args)
     line = {"metric": "Msamples/s, mixed batched workload (96 views, one launch per pass and hop depth)",
-            "value": batched["value"],
-            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "mixed-96-views", "spp_scale": args.spp_scale, "total_samples": total_samples,
-                       "passes_per_step": 16},
-            "batched": batched, "plain_per_view": plain, "wavefront_per_view": single,
-            "speedup_vs_plain": batched["value"] / plain["value"]}
+            "value": out["batched"]["value"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "config": {k: out[k] for k in ("workload", "spp_scale", "total_samples",
+                                                                "passes_per_step")}}
+    line.update({k: v for k, v in out.items() if k not in line["config"]})
     print(json.dumps(line), flush=True)
 
 
-def bench_serving(args):
+def measure_serving(args):
     """Poisson arrivals (70 % interactive 1280x720 8-spp frames with a moving camera, 30 %
     batch jobs drawn from the mixed workload), served by continuous batching under a 120 GB
     budget, against one-request-at-a-time plain kernels; p50/p99 latency per class."""
@@ -514,15 +597,23 @@ def bench_serving(args):
     for rate in [float(x) for x in args.rates.split(",")]:
         served = V.Server(ctx).run(V.make_requests(args.requests, rate))
         plain = V.plain_fifo(ctx, V.make_requests(args.requests, rate))
-        out[str(int(rate))] = {"served": served, "plain_fifo": plain}
+        out[str(int(rate))] = {"served": served, "plain_fifo": plain,
+                               "throughput_ratio": served["throughput_msamples_per_s"]
+                               / plain["throughput_msamples_per_s"]}
         torch.cuda.synchronize()
-    first = out[next(iter(out))]
+    return {"workload": "serving", "requests_per_rate": args.requests, "hbm_budget_gb": 120,
+            "interactive": "1280x720 x 8 spp hyperbolic, moving camera", "batch_spp_scale": 0.125,
+            "requests_stated": "10^4 requests per rate swept over 50-2000 req/s; this line runs "
+                               f"{args.requests} per rate at {args.rates} req/s", "rates": out}
+
+
+def bench_serving(args):
+    out = measure_serving(args)
+    first = out["rates"][next(iter(out["rates"]))]
     line = {"metric": "serving: throughput and p50/p99 frame latency, continuous batching vs plain per-request",
             "value": first["served"]["throughput_msamples_per_s"], "unit": UNIT, "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "serving", "requests_per_rate": args.requests, "hbm_budget_gb": 120,
-                       "interactive": "1280x720 x 8 spp hyperbolic, moving camera", "batch_spp_scale": 0.125},
-            "rates": out}
+            "config": {k: v for k, v in out.items() if k != "rates"}, "rates": out["rates"]}
     print(json.dumps(line), flush=True)
 
 

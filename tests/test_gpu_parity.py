@@ -23,6 +23,12 @@ ATOL_FLOOR = 1e-3
 # RTOL: both can only come from a branch that flipped on a last-ulp difference of a
 # transcendental (CUDA's logf / FP64 sincos / pow vs the host libm). Bound on their share:
 MAX_MISMATCH = 0.002
+# The same bound per executed hop, for runs long enough that flips compound along a pixel's
+# RNG stream: the GPU takes cos / sin (and log) in FP64 rounded once, the reference's host
+# build calls glibc's cosf / sinf, which round differently on a small share of arguments. In
+# the C restatement, swapping in the FP64-rounded cos / sin alone gives 0.3 % mismatched pixels
+# over 16 passes of the 1080p frame (about 76 hops per pixel): 4e-5 per hop. Bound: 1e-4.
+MAX_FLIP_PER_HOP = 1e-4
 
 
 def _compare(gpu_canvas, gpu_seeds, ref, label, min_exact=1.0 - MAX_MISMATCH, max_mismatch=MAX_MISMATCH):
@@ -87,7 +93,11 @@ def test_full_frame_config2_matches_reference(built):
     ref = oracle.render(wl.scene.to_bytes(), wl.scene.recipe, wl.scene.hops, W, H, pix, seeds0[pix],
                         passes=passes, threads=os.cpu_count() or 8, impl=impl, flags=oracle.JITTER_YX)
     assert ref.stats["samples"] == len(pix) * passes
-    _compare(cv[pix], sd[pix], ref, f"config2 full frame, {passes} passes, vs {impl}")
+    hops_per_pixel = ref.stats["hops"] / len(pix)
+    bound = 1.0 - (1.0 - MAX_FLIP_PER_HOP) ** hops_per_pixel
+    frac = _compare(cv[pix], sd[pix], ref, f"config2 full frame, {passes} passes, vs {impl}",
+                    min_exact=1.0 - bound, max_mismatch=bound)
+    print(f"hops per pixel {hops_per_pixel:.1f}, mismatch bound {bound:.4f}, flips per hop {frac / hops_per_pixel:.2e}")
 
 
 @pytest.mark.parametrize("cfg", ["config0", "config1"])
