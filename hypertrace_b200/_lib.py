@@ -23,6 +23,7 @@ HTC_RECIPE_EU = 2
 HTC_RECIPE_HY_TILED = 3
 HTC_RECIPE_EU_GRADIENT = 4
 HTC_RECIPE_CUSTOM = 100
+HTC_ERR_BUDGET = -5
 HTC_FLAG_JITTER_YX = 1
 
 STAT_SAMPLES, STAT_HOPS, STAT_OBJECT_TESTS, STAT_HITS = 0, 1, 2, 3
@@ -67,6 +68,14 @@ SIGNATURES = [
     ("htc_batch_graph_launch", _i, [_vp, _vp, _vp]),
     ("htc_batch_check", _i, [_vp, _vp]),
     ("htc_batch_reserve", _i, [_vp, ctypes.c_uint64, _u32, _vp]),
+    ("htc_serve_plan", _i, [_vp, _u32, ctypes.c_uint64, _vp]),
+    ("htc_server_create", _i, [ctypes.c_uint64, ctypes.c_uint64, _u32, ctypes.POINTER(_vp)]),
+    ("htc_server_destroy", None, [_vp]),
+    ("htc_server_configure", _i, [_vp, _u32, _u32, _u32, ctypes.c_uint64, _vp]),
+    ("htc_server_submit", _i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("htc_server_step", _i, [_vp, _vp, ctypes.POINTER(_u32)]),
+    ("htc_server_poll", _i, [_vp, _vp, _u32, ctypes.POINTER(_u32), _i]),
+    ("htc_server_stats", _i, [_vp, _vp]),
 ]
 
 
@@ -76,6 +85,33 @@ class HtcView(ctypes.Structure):
                 ("seeds", ctypes.c_void_p), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
                 ("recipe", ctypes.c_int32), ("light_hops", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("address_width", ctypes.c_int32), ("passes", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class HtcRequest(ctypes.Structure):
+    """struct htc_request (include/htcuda.h)."""
+    _fields_ = [("scene", ctypes.c_void_p), ("scene_size", ctypes.c_uint64), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("recipe", ctypes.c_int32), ("light_hops", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("address_width", ctypes.c_int32), ("passes", ctypes.c_uint32),
+                ("global_seed", ctypes.c_uint32), ("priority", ctypes.c_uint32), ("quantum", ctypes.c_uint32),
+                ("gamma", ctypes.c_float), ("reserved", ctypes.c_uint32), ("out_rgba8", ctypes.c_void_p),
+                ("out_canvas", ctypes.c_void_p), ("out_seeds", ctypes.c_void_p)]
+
+
+class HtcPlanItem(ctypes.Structure):
+    """struct htc_plan_item (include/htcuda.h)."""
+    _fields_ = [("pixels", ctypes.c_uint64), ("remaining", ctypes.c_uint32), ("quantum", ctypes.c_uint32),
+                ("priority", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class HtcServerInfo(ctypes.Structure):
+    """struct htc_server_info (include/htcuda.h)."""
+    _fields_ = [("waiting", ctypes.c_uint32), ("active", ctypes.c_uint32), ("in_flight", ctypes.c_uint32),
+                ("finished", ctypes.c_uint32), ("used_bytes", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64),
+                ("steps", ctypes.c_uint64)]
+
+
+HTC_PRIORITY_INTERACTIVE = 0
+HTC_PRIORITY_BATCH = 1
 
 
 class HtcError(RuntimeError):

@@ -14,7 +14,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRCS = [os.path.join(HERE, "csrc", "htcuda.cu"), os.path.join(HERE, "csrc", "htgeneric.cu")]
+SRCS = [os.path.join(HERE, "csrc", "htcuda.cu"), os.path.join(HERE, "csrc", "htgeneric.cu"),
+        os.path.join(HERE, "csrc", "htserve.cu")]
 OUT = os.path.join(HERE, "libhtcuda.so")
 # Device headers that htc_program_build hands to NVRTC, embedded as C strings.
 NVRTC_HEADERS = [("k_header_ht_math", "ht_math.cuh"), ("k_header_ht_generic", "ht_generic.cuh")]

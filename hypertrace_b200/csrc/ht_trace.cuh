@@ -119,15 +119,22 @@ HT_D bool mixture_interact(const Material &m, uint32_t &rng, V3 normal, V3 &dir,
     return false;
 }
 
-// Staged scene: inverse maps (2 x float4 per object) and shape indices in shared memory.
+// Staged scene, per slot in shared memory (hyperbolic scenes: planes first, then
+// horospheres, each in scene order; Euclidean scenes: slot = scene index).
 struct StagedScene {
-    const float4 *inv;       // shared, 2 per object
+    const float4 *inv;       // shared, 2 per slot
     const uint32_t *shape;   // shared
-    const float4 *bound;     // shared, 1 per object: world-space form for distance bounds
-    const float *mag;        // shared, 1 per object: BOUND_EPS * max |bound component|
+    const float4 *bound;     // shared, 1 per slot: world-space form for distance bounds
+    const float4 *pa, *pb;   // shared, per pair of slots: {x0, x1, y0, y1}, {z0, z1, w0, w1} of bound
+    const float2 *pmag;      // shared, per pair of slots: {mag0, mag1}
+    const float *mag;        // shared, 1 per slot: BOUND_EPS * max |bound component|
+    const uint32_t *orig;    // shared, 1 per slot: the object's index in the scene
     float4 *win;             // shared, this thread's 2 float4: the scan winner's local ray
-    const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials)
-    uint32_t n;
+    const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials), by scene index
+    uint32_t n;              // objects
+    uint32_t ns;             // slots: n, plus the dummy slot of a hyperbolic scene with an odd plane count
+    uint32_t n_planes;       // hyperbolic: slots [0, n_planes) are planes, horospheres from the next even slot
+    uint32_t dummy;          // the dummy slot, or 0xFFFFFFFF
     float fov;
     Col background;
     float4 cam0, cam1;       // camera map (Moebius or Homogenous3) as stored
@@ -330,13 +337,60 @@ HT_D Cull cull_none() {
     c.T = 1.0f;
     return c;
 }
-// Cheap bound: the distance from the ray start to the object alone (any hit lies on it).
-HT_D bool culled_point(float4 rec, float mag, uint32_t shape, const BoundRay &r, const Cull &c) {
-    const float t = r.t;
+// Cheap bound: the distance from the ray start to the object alone (any hit lies on it),
+// F = rec . (|p|^2, x, y, 1) with its error allowance eF:
+//   geodesic plane  culled when |F| - eF > 2 t S (sinh of the distance to the plane);
+//   horosphere      culled when t > E (F + eF) or t E < F - eF (the local height t' = t / F
+//                   outside [e^-thr, e^thr] even with F's error).
+// The point bound of two slots of one shape at once (packed FP32: each component rounds as the
+// scalar operation does). An object is culled when F + eF < lo or F - eF > hi:
+//   geodesic plane  lo = -2 t S, hi = 2 t S: the same decision as |F| - eF > 2 t S, op for
+//                   op (|F| - eF = -(F + eF) exactly when F < 0);
+//   horosphere      lo = t / E (E an upper bound of e^thr raised by 1e-5, so this stays below
+//                   t e^-thr after its rounding and the rcp approximation), hi = t E: the
+//                   test t > E (F + eF) or t E < F - eF with the division moved to the threshold.
+// A NaN record (ill-conditioned map) is never culled. Returns the survivors as bits 0 and 1.
+struct PointCut { float2 lo, hi; };
+HT_D PointCut point_cut(uint32_t shape, float t, const Cull &c) {
+    PointCut k;
+    if (shape == 0) {
+        const float h = 2.0f * t * c.S;
+        k.lo = make_float2(-h, -h);
+        k.hi = make_float2(h, h);
+    } else {
+        const float l = t * rcp_approx(c.E), h = t * c.E;
+        k.lo = make_float2(l, l);
+        k.hi = make_float2(h, h);
+    }
+    return k;
+}
+struct PairRay { float2 r2, x, y, K, nK; };   // the bound ray's constants, each in both halves
+HT_D PairRay pair_ray(const BoundRay &r) {
+    PairRay p;
+    p.r2 = make_float2(r.r2, r.r2);
+    p.x = make_float2(r.x, r.x);
+    p.y = make_float2(r.y, r.y);
+    p.K = make_float2(r.K, r.K);
+    p.nK = make_float2(-r.K, -r.K);
+    return p;
+}
+HT_D uint32_t survivors2(float4 a, float4 b, float2 mag, const PairRay &r, const PointCut &k) {
+    // F = rec.x r2 + (rec.y x + (rec.z y + rec.w)), as culled_point evaluates it
+    float2 F = __ffma2_rn(make_float2(b.x, b.y), r.y, make_float2(b.z, b.w));
+    F = __ffma2_rn(make_float2(a.z, a.w), r.x, F);
+    F = __ffma2_rn(make_float2(a.x, a.y), r.r2, F);
+    const float2 up = __fadd2_rn(F, __fmul2_rn(mag, r.K));     // F + eF
+    const float2 dn = __fadd2_rn(F, __fmul2_rn(mag, r.nK));    // F - eF (m (-K) = -(m K) exactly)
+    const bool c0 = up.x < k.lo.x || dn.x > k.hi.x;
+    const bool c1 = up.y < k.lo.y || dn.y > k.hi.y;
+    return (c0 ? 0u : 1u) | (c1 ? 0u : 2u);
+}
+HT_D bool culled_slot(const StagedScene &s, uint32_t q, const BoundRay &r, const PointCut &kp, const PointCut &kh) {
+    const float4 rec = s.bound[q];
     const float F = fmaf(rec.x, r.r2, fmaf(rec.y, r.x, fmaf(rec.z, r.y, rec.w)));
-    const float eF = bound_eF(mag, r);
-    if (shape == 0) return fabsf(F) - eF > 2.0f * t * c.S;
-    return t > c.E * (F + eF) || t * c.E < F - eF;
+    const float eF = s.mag[q] * r.K;
+    const PointCut &k = s.shape[q] == 0 ? kp : kh;
+    return F + eF < k.lo.x || F - eF > k.hi.x;
 }
 
 // true when object `rec` provably cannot be hit nearer than the current threshold
@@ -441,73 +495,91 @@ HT_D float sure_crossing_e2(const BoundFW &b, uint32_t shape, bool plane_repeat,
 // Distance of a crossing from its e^(2 s) bound (the threshold built from it adds 1e-2 margins).
 HT_D float dist_from_e2(float x) { return 0.5f * LN2F * lg2_approx(x); }
 
-// Upper estimate of the nearest hit among objects [0, n) that the reference surely reports
-// (the least sure_crossing_e2), +inf when none qualifies. A threshold derived from it
+// Upper estimate of the nearest hit that the reference surely reports (the least
+// sure_crossing_e2) among the first HT_EST_OBJECTS / 2 planes and the first HT_EST_OBJECTS / 2
+// horospheres of the staged slots, +inf when none qualifies. A threshold derived from it
 // (cull_from_dist) then culls before the first exact test.
-HT_D float upper_estimate(const StagedScene &s, uint32_t n, const BoundRay &r, uint32_t prev_hash) {
-    float best = __int_as_float(0x7f800000);
-    for (uint32_t k = 0; k < n; ++k)   // warp-uniform: broadcast loads
-        best = fminf(best, sure_crossing_e2(bound_fw(s.bound[k], s.mag[k], r), s.shape[k], k == prev_hash, r.t));
+HT_D float est_range(const StagedScene &s, uint32_t q0, uint32_t q1, const BoundRay &r, uint32_t prev_hash, float best) {
+    for (uint32_t q = q0; q < q1; ++q)   // warp-uniform: broadcast loads
+        best = fminf(best, sure_crossing_e2(bound_fw(s.bound[q], s.mag[q], r), s.shape[q], s.orig[q] == prev_hash, r.t));
+    return best;
+}
+HT_D float upper_estimate(const StagedScene &s, const BoundRay &r, uint32_t prev_hash) {
+    const uint32_t half = HT_EST_OBJECTS / 2, h0 = (s.n_planes + 1) & ~1u;
+    float best = est_range(s, 0, min(half, s.n_planes), r, prev_hash, __int_as_float(0x7f800000));
+    best = est_range(s, h0, min(h0 + half, s.ns), r, prev_hash, best);
     return best < __int_as_float(0x7f800000) ? dist_from_e2(best) : best;
 }
 
 template <bool OOL>
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
                  Col &intensity, Col &emission, bool &hit, uint32_t &n_exact) {
-    // Nearest hit with ties to the lowest index (object/vector.inl:37-50), comparing
-    // x = cosh(distance) and taking the logarithm only when x can win, and skipping
-    // objects whose distance bound rules them out.
+    // Nearest hit with ties to the lowest scene index (object/vector.inl:37-50): candidates
+    // are compared on (distance, index), so the order of the slots does not matter; x =
+    // cosh(distance) is compared first and the logarithm taken only when x can win; objects
+    // whose distance bound rules them out are not tested.
     float min_dist = -1.0f;
     float min_x = __int_as_float(0x7f800000);   // +inf
-    uint32_t kmin = 0;
+    uint32_t kmin = 0, kmin_orig = 0xFFFFFFFFu;
     const Q4 p = ray.p, v = ray.v;
     const bool can_cull = cull_point_ok(p);
     const BoundRay br = bound_ray(p, v);
+    const PairRay pr = pair_ray(br);
     Cull cull = cull_none();
-    if (can_cull) {   // a threshold before the first exact test, from the first chunk's crossings
-        const float u = upper_estimate(s, min(HT_EST_OBJECTS, s.n), br, prev_hash);
+    if (can_cull) {   // a threshold before the first exact test, from the first slots' crossings
+        const float u = upper_estimate(s, br, prev_hash);
         if (u < __int_as_float(0x7f800000)) cull = cull_from_dist(u);
     }
-    for (uint32_t c0 = 0; c0 < s.n; c0 += 32) {
-        const uint32_t cn = min(32u, s.n - c0);
-        uint32_t mask = 0;
-        // kept rolled: the kernel is bound by instruction fetch as much as by issue (unrolled
-        // by 8: 7.06 ms per pass at 1080p / 200 objects, fully: 9.43, rolled: 6.24)
+    PointCut kp = point_cut(0, br.t, cull), kh = point_cut(1, br.t, cull);
+    for (uint32_t c0 = 0; c0 < s.ns; c0 += 32) {
+        const uint32_t cn = min(32u, s.ns - c0);
+        uint32_t valid = cn == 32 ? 0xFFFFFFFFu : (1u << cn) - 1u;
+        if (s.dummy - c0 < 32u) valid &= ~(1u << (s.dummy - c0));
+        uint32_t mask = valid;
+        if (can_cull) {
+            mask = 0;
+            // kept rolled: the kernel is bound by instruction fetch as much as by issue
 #pragma unroll 1
-        for (uint32_t j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads, cheap bound
-            const uint32_t k = c0 + j;
-            if (!can_cull || !culled_point(s.bound[k], s.mag[k], s.shape[k], br, cull)) mask |= 1u << j;
-        }
-        if (can_cull) {   // per lane: the ray-aware bound on the survivors only
+            for (uint32_t j = 0; j < cn; j += 2) {   // warp-uniform: broadcast loads, two slots at once
+                const uint32_t pq = (c0 + j) >> 1;
+                const PointCut &k = c0 + j >= s.n_planes ? kh : kp;
+                mask |= survivors2(s.pa[pq], s.pb[pq], s.pmag[pq], pr, k) << j;
+            }
+            mask &= valid;
+            // per lane: the ray-aware bound on the survivors only
             uint32_t m = mask;
             while (m) {
                 const uint32_t j = __ffs(m) - 1;
                 m &= m - 1;
-                const uint32_t k = c0 + j;
-                if (culled<OOL>(s.bound[k], s.mag[k], s.shape[k], br, cull)) mask &= ~(1u << j);
+                const uint32_t q = c0 + j;
+                if (culled<OOL>(s.bound[q], s.mag[q], s.shape[q], br, cull)) mask &= ~(1u << j);
             }
         }
-        while (mask) {   // this lane's candidates, in index order
-            const uint32_t k = c0 + (__ffs(mask) - 1);
+        while (mask) {   // this lane's candidates, in slot order
+            const uint32_t q = c0 + (__ffs(mask) - 1);
             mask &= mask - 1;
-            const uint32_t shape = s.shape[k];
-            if (can_cull && culled_point(s.bound[k], s.mag[k], shape, br, cull)) continue;
+            const uint32_t shape = s.shape[q];
+            if (can_cull && culled_slot(s, q, br, kp, kh)) continue;
+            const uint32_t k = s.orig[q];
             const bool repeat = (k == prev_hash);
             if (shape == 0 && repeat) continue;   // a geodesic plane is never hit twice in a row
             ++n_exact;
             // the out-of-line copy of the map, shared with the hit path: one copy of its code
             // (the kernel is bound by instruction fetch as much as by issue)
-            HyRay l = ray_hy_map_call(mo_from(s.inv[2 * k], s.inv[2 * k + 1]), p, v);
+            HyRay l = ray_hy_map_call(mo_from(s.inv[2 * q], s.inv[2 * q + 1]), p, v);
             const float x = shape == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, repeat);
-            // candidates come in index order, so x above the best's cannot win (its distance
-            // is not smaller, and a tie keeps the lower index)
-            if (x >= 1.0f && x <= min_x) {
+            // x above the best's gives a distance no smaller (hy_dist_from_x is non-decreasing),
+            // which can only win a tie, and only from a lower scene index
+            if (x >= 1.0f && (x <= min_x || k < kmin_orig)) {
                 const float dist = hy_dist_from_x(x);
-                if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+                if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist || (dist == min_dist && k < kmin_orig))) {
                     min_dist = dist;
                     min_x = x;
-                    kmin = k;
+                    kmin = q;
+                    kmin_orig = k;
                     cull = cull_from_dist(dist);
+                    kp = point_cut(0, br.t, cull);
+                    kh = point_cut(1, br.t, cull);
                     s.win[0] = make_float4(l.p.x, l.p.y, l.p.z, l.p.w);   // kept for the hit
                     s.win[1] = make_float4(l.v.x, l.v.y, l.v.z, l.v.w);
                 }
@@ -523,9 +595,9 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     }
     hit = true;
     const Mo inv = mo_from(s.inv[2 * kmin], s.inv[2 * kmin + 1]);
-    const uint8_t *obj = s.objects + (size_t)kmin * OBJ_STRIDE;
+    const uint8_t *obj = s.objects + (size_t)kmin_orig * OBJ_STRIDE;
     const Mo fwd = load_mo(obj);
-    const bool repeat = (kmin == prev_hash);
+    const bool repeat = (kmin_orig == prev_hash);
     HyRay l;   // the winner's local ray, as the scan computed it (the same map, the same bits)
     {
         const float4 a = s.win[0], b = s.win[1];
@@ -545,7 +617,7 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     ray.p = out.p;
     ray.v = out.v;
     if (!ret) return false;
-    prev_hash = kmin;   // the hasher state after hash_usize(0, index) is the index
+    prev_hash = kmin_orig;   // the hasher state after hash_usize(0, index) is the index
     return true;
 }
 

@@ -77,40 +77,89 @@ struct htc_program {
     void *wave_buf;            // two wavefront queues (WAVE_SLOT_BYTES per slot each), grown on demand
     size_t wave_slots;         // slots per queue
     uint32_t *d_wave_ctr;      // 2 counters per hop depth
+    int double_support;        // scene bytes in the double_support layout, narrowed before rendering
+    uint8_t *narrow_buf;       // the narrowed (f32 layout) scene, grown on demand
+    size_t narrow_bytes;
 };
 
 // ============================================================================ staging
-// Loads the scene header and the inverse maps / shape indices of every object into shared
-// memory. Returns false (uniformly across the block) when the scene bytes fail validation.
-// Shared-memory layout of a staged scene of up to n objects (smem_bytes(n) bytes): inverse
-// maps (2 float4), bound records (float4), shape indices (u32), bound magnitudes (f32) per
-// object, then 2 float4 per thread of a 128-thread block (the scan's winner, local frame).
+// Loads the scene header and the per-object data the scan reads into shared memory. Returns
+// false (uniformly across the block) when the scene bytes fail validation.
+//
+// Hyperbolic scenes are staged in scan order, geodesic planes first (in index order), then
+// horospheres (in index order); when the plane count is odd a dummy slot follows the planes,
+// so that every pair of slots (2p, 2p + 1) holds one shape and the point-bound loop can test
+// two objects per packed FP32 instruction. `orig[slot]` is the object's index in the scene:
+// the scan compares hits on (distance, index), the reference's nearest-hit rule
+// (object/vector.inl:37-50), so the order of the slots never changes the winner. Euclidean
+// scenes are staged in index order (slot = index).
+//
+// Shared-memory layout for up to n objects (n + 1 slots, smem_bytes(n) bytes): inverse maps
+// (2 float4 per slot), bound records (float4), the bound records again as pairs of slots
+// ({x0, x1, y0, y1}, {z0, z1, w0, w1} per pair) and their magnitudes ({m0, m1}), then shape,
+// bound magnitude and scene index per slot (u32 / f32 / u32), then 2 float4 per thread of a
+// 128-thread block (the scan's winner, local frame).
 constexpr uint32_t BLOCK_THREADS = 128;
 struct SceneSmem {
-    float4 *inv, *bound;
-    uint32_t *shape;
+    float4 *inv, *bound, *pa, *pb;
+    float2 *pmag;
+    uint32_t *shape, *orig;
     float *mag;
     float4 *win;
     float4 *end;   // first float4 past the layout
 };
-__host__ __device__ constexpr size_t scene_win_offset(uint32_t n) { return ((size_t)n * 56u + 15u) & ~(size_t)15u; }
+__host__ __device__ constexpr uint32_t scene_slots(uint32_t n) { return n + 1; }
+__host__ __device__ constexpr size_t scene_win_offset(uint32_t n) {
+    return ((size_t)scene_slots(n) * 60u + (size_t)((scene_slots(n) + 1) / 2) * 40u + 15u) & ~(size_t)15u;
+}
 __device__ __forceinline__ SceneSmem carve_scene(float4 *smem, uint32_t n) {
+    const uint32_t ns = scene_slots(n), np = (ns + 1) / 2;
     SceneSmem c;
     c.inv = smem;
-    c.bound = smem + 2 * n;
-    c.shape = reinterpret_cast<uint32_t *>(smem + 3 * n);
-    c.mag = reinterpret_cast<float *>(c.shape + n);
+    c.bound = c.inv + 2 * ns;
+    c.pa = c.bound + ns;
+    c.pb = c.pa + np;
+    c.pmag = reinterpret_cast<float2 *>(c.pb + np);
+    c.shape = reinterpret_cast<uint32_t *>(c.pmag + np);
+    c.mag = reinterpret_cast<float *>(c.shape + ns);
+    c.orig = reinterpret_cast<uint32_t *>(c.mag + ns);
     c.win = smem + scene_win_offset(n) / 16;
     c.end = c.win + 2 * BLOCK_THREADS;
     return c;
+}
+
+// Stages object k (shape `shape`) into slot q.
+template <int R>
+__device__ __forceinline__ void stage_object(const uint8_t *obj, uint32_t shape, uint32_t k, uint32_t q,
+                                             const SceneSmem &sm) {
+    sm.shape[q] = shape;
+    sm.orig[q] = k;
+    float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float mag = 0.0f;
+    if (R == RECIPE_HY) {
+        const Mo fwd = load_mo(obj);
+        Mo inv = mo_inverse(fwd);
+        sm.inv[2 * q] = make_float4(inv.a.x, inv.a.y, inv.b.x, inv.b.y);
+        sm.inv[2 * q + 1] = make_float4(inv.c.x, inv.c.y, inv.d.x, inv.d.y);
+        rec = stage_bound(fwd, shape);
+        mag = bound_mag(rec);
+    } else {
+        Hom inv = hom3_inverse(load_hom(obj));
+        sm.inv[2 * q] = make_float4(inv.shift.x, inv.shift.y, inv.shift.z, 0.0f);
+        sm.inv[2 * q + 1] = make_float4(inv.rot.x, inv.rot.y, inv.rot.z, inv.rot.w);
+    }
+    sm.bound[q] = rec;
+    sm.mag[q] = mag;
+    float *pa = reinterpret_cast<float *>(&sm.pa[q >> 1]), *pb = reinterpret_cast<float *>(&sm.pb[q >> 1]);
+    const uint32_t o = q & 1u;
+    pa[o] = rec.x; pa[2 + o] = rec.y; pb[o] = rec.z; pb[2 + o] = rec.w;
+    reinterpret_cast<float *>(&sm.pmag[q >> 1])[o] = mag;
 }
 
 template <int R>
 __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t max_objects,
                             int address_width, uint32_t *err, StagedScene &s, const SceneSmem &sm,
                             uint32_t *s_hdr) {
-    float4 *s_inv = sm.inv, *s_bound = sm.bound;
-    uint32_t *s_shape = sm.shape;
     using L = Layout<R>;
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         uint32_t ok = 1;
@@ -135,26 +184,63 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
     }
     const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
     const uint32_t nthreads = blockDim.x * blockDim.y;
+    const uint8_t *objects = scene + L::OBJECTS;
     bool bad = false;
-    for (uint32_t k = tid; k < n; k += nthreads) {
-        const uint8_t *obj = scene + L::OBJECTS + (size_t)k * OBJ_STRIDE;
-        uint32_t shape = ldu(obj, O_SHAPE);
-        if (address_width == 64 && ldu(obj, O_SHAPE + 4) != 0) bad = true;
-        if (shape > 1) bad = true;
-        s_shape[k] = shape;
-        if (R == RECIPE_HY) {
-            const Mo fwd = load_mo(obj);
-            Mo inv = mo_inverse(fwd);
-            s_inv[2 * k] = make_float4(inv.a.x, inv.a.y, inv.b.x, inv.b.y);
-            s_inv[2 * k + 1] = make_float4(inv.c.x, inv.c.y, inv.d.x, inv.d.y);
-            const float4 rec = stage_bound(fwd, shape);
-            s_bound[k] = rec;
-            sm.mag[k] = bound_mag(rec);
-        } else {
-            Hom inv = hom3_inverse(load_hom(obj));
-            s_inv[2 * k] = make_float4(inv.shift.x, inv.shift.y, inv.shift.z, 0.0f);
-            s_inv[2 * k + 1] = make_float4(inv.rot.x, inv.rot.y, inv.rot.z, inv.rot.w);
-            sm.mag[k] = 0.0f;
+    uint32_t n_planes = 0, dummy = 0xFFFFFFFFu;
+    if (R == RECIPE_HY) {
+        // pass 1: the number of planes
+        for (uint32_t r0 = 0; r0 < n; r0 += nthreads) {
+            const uint32_t k = r0 + tid;
+            const bool plane = k < n && ldu(objects + (size_t)k * OBJ_STRIDE, O_SHAPE) == 0;
+            n_planes += (uint32_t)__syncthreads_count(plane ? 1 : 0);
+        }
+        // pass 2: slot = rank among the planes, or n_planes (rounded up to even) + rank among
+        // the horospheres; ranks from a ballot per warp and the warps' counts in s_hdr[2..]
+        const uint32_t h0 = (n_planes + 1) & ~1u;
+        const uint32_t lane = tid & 31u, warp = tid >> 5, nwarps = (nthreads + 31) >> 5;
+        uint32_t before = 0;   // planes before this round
+        for (uint32_t r0 = 0; r0 < n; r0 += nthreads) {
+            const uint32_t k = r0 + tid;
+            const bool in = k < n;
+            const uint8_t *obj = objects + (size_t)k * OBJ_STRIDE;
+            const uint32_t shape = in ? ldu(obj, O_SHAPE) : 1u;
+            const uint32_t ballot = __ballot_sync(0xffffffffu, in && shape == 0);
+            if (lane == 0) s_hdr[2 + warp] = (uint32_t)__popc(ballot);
+            __syncthreads();
+            uint32_t rank = before + (uint32_t)__popc(ballot & ((1u << lane) - 1u)), total = 0;
+            for (uint32_t w = 0; w < nwarps; ++w) {
+                const uint32_t c = s_hdr[2 + w];
+                if (w < warp) rank += c;
+                total += c;
+            }
+            __syncthreads();
+            before += total;
+            if (in) {
+                if (address_width == 64 && ldu(obj, O_SHAPE + 4) != 0) bad = true;
+                if (shape > 1) bad = true;
+                stage_object<R>(obj, shape > 1 ? 1u : shape, k, shape == 0 ? rank : h0 + (k - rank), sm);
+            }
+        }
+        if (n_planes & 1u) {   // the dummy slot: never a candidate (masked), NaN bound record
+            dummy = n_planes;
+            if (tid == 0) {
+                const float nan = __int_as_float(0x7fc00000);
+                sm.shape[dummy] = 0;
+                sm.orig[dummy] = 0xFFFFFFFFu;
+                sm.bound[dummy] = make_float4(nan, nan, nan, nan);
+                sm.mag[dummy] = 0.0f;
+                float *pa = reinterpret_cast<float *>(&sm.pa[dummy >> 1]), *pb = reinterpret_cast<float *>(&sm.pb[dummy >> 1]);
+                pa[1] = 0.0f; pa[3] = 0.0f; pb[1] = 0.0f; pb[3] = 0.0f;   // the odd half of its pair
+                reinterpret_cast<float *>(&sm.pmag[dummy >> 1])[1] = 0.0f;
+            }
+        }
+    } else {
+        for (uint32_t k = tid; k < n; k += nthreads) {
+            const uint8_t *obj = objects + (size_t)k * OBJ_STRIDE;
+            const uint32_t shape = ldu(obj, O_SHAPE);
+            if (address_width == 64 && ldu(obj, O_SHAPE + 4) != 0) bad = true;
+            if (shape > 1) bad = true;
+            stage_object<R>(obj, shape > 1 ? 1u : shape, k, k, sm);
         }
     }
     const int any_bad = __syncthreads_or(bad ? 1 : 0);
@@ -162,13 +248,20 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
         if (tid == 0) atomicOr(err, ERR_SCENE);
         return false;
     }
-    s.inv = s_inv;
-    s.bound = s_bound;
-    s.shape = s_shape;
+    s.inv = sm.inv;
+    s.bound = sm.bound;
+    s.pa = sm.pa;
+    s.pb = sm.pb;
+    s.pmag = sm.pmag;
+    s.shape = sm.shape;
     s.mag = sm.mag;
+    s.orig = sm.orig;
     s.win = sm.win + 2 * tid;
-    s.objects = scene + L::OBJECTS;
+    s.objects = objects;
     s.n = n;
+    s.ns = n + (dummy != 0xFFFFFFFFu ? 1u : 0u);
+    s.n_planes = R == RECIPE_HY ? n_planes : 0u;
+    s.dummy = dummy;
     s.fov = ldf(scene, L::FOV);
     float4 bg = ldf4(scene, L::BG);
     s.background.x = bg.x; s.background.y = bg.y; s.background.z = bg.z;
@@ -229,7 +322,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_plain(
     uint32_t W, uint32_t H, uint32_t hops, uint32_t flags, float4 *__restrict__ canvas,
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err) {
     extern __shared__ float4 smem[];
-    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_hdr[2 + BLOCK_THREADS / 32];
     const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
     if (!stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, sm, s_hdr)) return;
@@ -389,7 +482,7 @@ __global__ void __launch_bounds__(128, HT_PERSIST_MINB) render_persistent(
     float4 *__restrict__ canvas, uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err,
     uint32_t *queue) {
     extern __shared__ float4 smem[];
-    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_hdr[2 + BLOCK_THREADS / 32];
     const SceneSmem sm = carve_scene(smem, max_objects);
     StagedScene s;
     const bool staged = stage_scene<R>(scene, scene_size, max_objects, address_width, err, s, sm, s_hdr);
@@ -525,7 +618,7 @@ __global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err, WaveQueue in, const uint32_t *in_count,
     WaveQueue out, uint32_t *ctr) {
     extern __shared__ float4 smem[];
-    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_hdr[2 + BLOCK_THREADS / 32];
     const uint32_t n = FH == 1 ? W * H : *reinterpret_cast<const volatile uint32_t *>(in_count);
     if (n == 0 || blockIdx.x * 128u >= n) return;   // nothing for this block: skip the staging
     const SceneSmem sm = carve_scene(smem, max_objects);
@@ -584,7 +677,7 @@ __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) ren
     uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
     uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err) {
     extern __shared__ float4 smem[];
-    __shared__ uint32_t s_hdr[2];
+    __shared__ uint32_t s_hdr[2 + BLOCK_THREADS / 32];
     __shared__ uint32_t s_tile, s_next, s_total, s_tsize;
     __shared__ int s_staged_view, s_staged_ok;
     const SceneSmem sm = carve_scene(smem, smem_objects);
@@ -694,6 +787,78 @@ __global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) ren
         }
     }
     flush_lane_stats(stats, st);
+}
+
+// ============================================================================ double_support
+// A scene serialized with double_support (types/src/config.rs:38-43) stores every f64 field
+// in 8 bytes, and a primitive vector or matrix of f64 is aligned to its own size
+// (types/src/primitive/scalar.rs:186-215, types/src/primitive/matrix.rs:171-209); colors stay
+// f32. The reference then builds its kernel with real = double (processing/src/render.rs:50).
+// This path narrows such a scene once per render call into the f32 layout the kernels read,
+// rounding each f64 to the nearest f32 -- the value the reference's own serializer writes for
+// the same scene without double_support (`*self as f32`, scalar.rs:198-207) -- and then
+// transports in FP32 as for any other scene: a double_support scene renders bit for bit as
+// its f32 serialization does. The field tables follow the layouts hypertrace_b200/types.py
+// derives (Moebius 8 reals, Shift3 3 + 1, Rotation3 4, fov and portions 1).
+struct NarrowField { uint16_t src, dst; uint8_t kind, n; };   // kind: 0 = n f64 -> f32, 1 = n words, 2 = usize
+struct NarrowLayout {
+    uint32_t src_objects, src_stride, dst_objects, dst_stride, src_count, dst_count;
+    uint32_t n_header, n_object;
+    NarrowField header[5], object[8];
+};
+__constant__ NarrowLayout c_narrow[2] = {
+    // HTC_RECIPE_HY: view map, fov, background | map, diffuse color / portion, specular portion,
+    // emission, luminous portion, shape index
+    {256, 192, 128, 128, 192, 96, 3, 7,
+     {{0, 0, 0, 8}, {64, 32, 0, 1}, {128, 64, 1, 3}},
+     {{0, 0, 0, 8}, {64, 32, 1, 3}, {80, 48, 0, 1}, {96, 64, 0, 1}, {112, 80, 1, 3}, {128, 96, 0, 1}, {144, 112, 2, 1}}},
+    // HTC_RECIPE_EU: view shift, rotation, fov, background | shift, rotation, diffuse color /
+    // portion, specular portion, emission, luminous portion, shape index
+    {160, 160, 80, 128, 128, 64, 4, 8,
+     {{0, 0, 0, 3}, {32, 16, 0, 4}, {64, 32, 0, 1}, {96, 48, 1, 3}},
+     {{0, 0, 0, 3}, {32, 16, 0, 4}, {64, 32, 1, 3}, {80, 48, 0, 1}, {96, 64, 0, 1}, {112, 80, 1, 3}, {128, 96, 0, 1},
+      {144, 112, 2, 1}}},
+};
+constexpr uint32_t NARROW_SRC_OBJECTS[2] = {256, 160}, NARROW_SRC_STRIDE[2] = {192, 160};
+
+__device__ __forceinline__ void narrow_fields(const uint8_t *src, uint8_t *dst, const NarrowField *f, uint32_t nf,
+                                              int usize_bytes) {
+    for (uint32_t i = 0; i < nf; ++i) {
+        const NarrowField fd = f[i];
+        if (fd.kind == 0) {
+            const double *a = reinterpret_cast<const double *>(src + fd.src);
+            float *b = reinterpret_cast<float *>(dst + fd.dst);
+            for (uint32_t j = 0; j < fd.n; ++j) b[j] = __double2float_rn(a[j]);
+        } else {
+            const uint32_t words = fd.kind == 1 ? fd.n : (uint32_t)usize_bytes / 4u;
+            const uint32_t *a = reinterpret_cast<const uint32_t *>(src + fd.src);
+            uint32_t *b = reinterpret_cast<uint32_t *>(dst + fd.dst);
+            for (uint32_t j = 0; j < words; ++j) b[j] = a[j];
+        }
+    }
+}
+// One thread per record (record 0 = the header, record 1 + i = object i). An object count the
+// source buffer cannot hold (or the destination was not sized for) is written as all ones,
+// which the render's own staging rejects as a scene error.
+__global__ void k_narrow_scene(int li, const uint8_t *__restrict__ src, uint64_t src_size, uint8_t *__restrict__ dst,
+                               uint32_t dst_capacity, int usize_bytes) {
+    const NarrowLayout &L = c_narrow[li];
+    const uint32_t count_lo = *reinterpret_cast<const uint32_t *>(src + L.src_count);
+    const uint32_t count_hi = usize_bytes == 8 ? *reinterpret_cast<const uint32_t *>(src + L.src_count + 4) : 0u;
+    const uint64_t holds = src_size >= L.src_objects ? (src_size - L.src_objects) / L.src_stride : 0u;
+    const bool ok = count_hi == 0 && count_lo <= holds && count_lo <= dst_capacity;
+    const uint32_t n = ok ? count_lo : 0u;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += gridDim.x * blockDim.x) {
+        if (r == 0) {
+            narrow_fields(src, dst, L.header, L.n_header, usize_bytes);
+            uint32_t *c = reinterpret_cast<uint32_t *>(dst + L.dst_count);
+            c[0] = ok ? count_lo : 0xFFFFFFFFu;
+            if (usize_bytes == 8) c[1] = ok ? 0u : 0xFFFFFFFFu;
+        } else {
+            narrow_fields(src + L.src_objects + (size_t)(r - 1) * L.src_stride,
+                          dst + L.dst_objects + (size_t)(r - 1) * L.dst_stride, L.object, L.n_object, usize_bytes);
+        }
+    }
 }
 
 // ============================================================================ post
@@ -855,8 +1020,9 @@ int htc_program_create(int recipe, uint32_t light_hops, int address_width, int d
         return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
     if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
     if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
-    if (double_support) return fail(HTC_ERR_UNSUPPORTED, "double_support scenes are not served (f32 transport)");
     if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    if (double_support && recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU)
+        return fail(HTC_ERR_UNSUPPORTED, "double_support scenes are served for HTC_RECIPE_HY and HTC_RECIPE_EU only");
     if (recipe == HTC_RECIPE_HY_TILED || recipe == HTC_RECIPE_EU_GRADIENT) {
         GenericProgram *g = nullptr;
         int rc = generic_program_create(recipe, address_width, &g);
@@ -870,6 +1036,7 @@ int htc_program_create(int recipe, uint32_t light_hops, int address_width, int d
     p->hops = light_hops;
     p->address_width = address_width;
     p->flags = flags;
+    p->double_support = double_support ? 1 : 0;
     cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_err, sizeof(uint32_t));
@@ -900,6 +1067,7 @@ void htc_program_destroy(htc_program *p) {
     if (p->d_queue) cudaFree(p->d_queue);
     if (p->wave_buf) cudaFree(p->wave_buf);
     if (p->d_wave_ctr) cudaFree(p->d_wave_ctr);
+    if (p->narrow_buf) cudaFree(p->narrow_buf);
     if (p->generic) generic_program_destroy(p->generic);
     delete p;
 }
@@ -923,6 +1091,7 @@ int htc_program_static_size(const htc_program *p, uint64_t *bytes) {
     if (rc) return rc;
     if (!bytes) return fail(HTC_ERR_INVALID, "bytes is NULL");
     if (p->generic) *bytes = generic_min_size(p->generic);
+    else if (p->double_support) *bytes = NARROW_SRC_OBJECTS[p->recipe == HTC_RECIPE_HY ? 0 : 1];
     else *bytes = p->recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
     return HTC_OK;
 }
@@ -982,8 +1151,42 @@ static int render_generic_program(htc_program *p, uint32_t W, uint32_t H, const 
                           p->d_err, stream);
 }
 
-int htc_render_ex(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
-                  float *canvas, uint32_t *seeds, uint64_t *stats, void *stream) {
+}  // extern "C"
+
+// A double_support program's scene, narrowed on `stream` into the program's f32-layout buffer
+// (k_narrow_scene); *scene / *scene_size then name that buffer. Other programs: unchanged.
+static int narrow_scene(htc_program *p, const void **scene, size_t *scene_size, void *stream) {
+    if (!p || !p->double_support) return HTC_OK;
+    const int li = p->recipe == HTC_RECIPE_HY ? 0 : 1;
+    if (!*scene) return fail(HTC_ERR_INVALID, "scene must be a device pointer");
+    if ((reinterpret_cast<uintptr_t>(*scene) & 15u) != 0) return fail(HTC_ERR_INVALID, "scene must be 16-byte aligned");
+    if (*scene_size < NARROW_SRC_OBJECTS[li])
+        return fail(HTC_ERR_SCENE, "scene buffer is smaller than the scene header (double_support layout)");
+    uint64_t cap = (*scene_size - NARROW_SRC_OBJECTS[li]) / NARROW_SRC_STRIDE[li];
+    if (cap > 0xFFFFFFull) cap = 0xFFFFFFull;
+    const size_t dst_objects = li == 0 ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
+    const size_t bytes = dst_objects + (size_t)cap * OBJ_STRIDE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (p->narrow_bytes < bytes) {
+        if (p->narrow_buf) HTC_CUDA(cudaFree(p->narrow_buf));
+        p->narrow_buf = nullptr;
+        p->narrow_bytes = 0;
+        HTC_CUDA(cudaMalloc(&p->narrow_buf, bytes));
+        HTC_CUDA(cudaMemsetAsync(p->narrow_buf, 0, bytes, st));   // the layout's padding
+        p->narrow_bytes = bytes;
+    }
+    const uint32_t records = (uint32_t)cap + 1u;
+    const unsigned blocks = std::min<unsigned>((records + 127u) / 128u, 148u * 8u);
+    k_narrow_scene<<<blocks, 128, 0, st>>>(li, reinterpret_cast<const uint8_t *>(*scene), *scene_size, p->narrow_buf,
+                                           (uint32_t)cap, p->address_width / 8);
+    HTC_CUDA(cudaGetLastError());
+    *scene = p->narrow_buf;
+    *scene_size = bytes;
+    return HTC_OK;
+}
+
+static int render_ex_impl(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                          float *canvas, uint32_t *seeds, uint64_t *stats, void *stream) {
     if (p && p->generic) return render_generic_program(p, W, H, scene, scene_size, canvas, seeds, 1, stats, stream);
     uint32_t max_objects = 0;
     size_t smem = 0;
@@ -1001,6 +1204,17 @@ int htc_render_ex(htc_program *p, uint32_t W, uint32_t H, const void *scene, siz
                                                          p->hops, p->flags, cv, seeds, stats, p->d_err);
     HTC_CUDA(cudaGetLastError());
     return HTC_OK;
+}
+
+extern "C" {
+
+int htc_render_ex(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                  float *canvas, uint32_t *seeds, uint64_t *stats, void *stream) {
+    if (p && canvas && seeds && W && H) {   // argument errors are reported by the render checks
+        int rc = narrow_scene(p, &scene, &scene_size, stream);
+        if (rc) return rc;
+    }
+    return render_ex_impl(p, W, H, scene, scene_size, canvas, seeds, stats, stream);
 }
 
 int htc_render(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size, float *canvas,
@@ -1067,8 +1281,10 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
 
 extern "C" {
 
-int htc_render_wavefront(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
-                         float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+}  // extern "C"
+
+static int render_wavefront_impl(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                                 float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
     if (p && p->generic) return fail(HTC_ERR_UNSUPPORTED, "the wavefront form serves the built-in recipes only");
     uint32_t max_objects = 0;
     size_t smem = 0;
@@ -1085,9 +1301,24 @@ int htc_render_wavefront(htc_program *p, uint32_t W, uint32_t H, const void *sce
     return launch_wave<RECIPE_EU>(p, W, H, sc, scene_size, max_objects, smem, cv, seeds, passes, stats, st);
 }
 
+extern "C" {
+
+int htc_render_wavefront(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
+                         float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
+    if (p && canvas && seeds && W && H && passes) {
+        int rc = narrow_scene(p, &scene, &scene_size, stream);
+        if (rc) return rc;
+    }
+    return render_wavefront_impl(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
+}
+
 int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene, size_t scene_size,
                       float *canvas, uint32_t *seeds, uint32_t passes, uint64_t *stats, void *stream) {
     if (p && p->generic) return render_generic_program(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
+    if (p && canvas && seeds && W && H && passes) {
+        int rc = narrow_scene(p, &scene, &scene_size, stream);
+        if (rc) return rc;
+    }
     uint32_t max_objects = 0;
     size_t smem = 0;
     int rc = validate_render_args(p, W, H, scene, scene_size, canvas, seeds, &max_objects, &smem);
@@ -1099,10 +1330,10 @@ int htc_render_passes(htc_program *p, uint32_t W, uint32_t H, const void *scene,
     // wavefronts). Either way the result is the same bits.
     const bool cheap = (uint64_t)W * H < (1u << 19) && (p->recipe == HTC_RECIPE_EU || max_objects < 100);
     if (HT_PASSES_MODE == 2 && !cheap)
-        return htc_render_wavefront(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
+        return render_wavefront_impl(p, W, H, scene, scene_size, canvas, seeds, passes, stats, stream);
     if (HT_PASSES_MODE == 0 || HT_PASSES_MODE == 2) {
         for (uint32_t k = 0; k < passes; ++k) {
-            int rc2 = htc_render_ex(p, W, H, scene, scene_size, canvas, seeds, stats, stream);
+            int rc2 = render_ex_impl(p, W, H, scene, scene_size, canvas, seeds, stats, stream);
             if (rc2) return rc2;
         }
         return HTC_OK;

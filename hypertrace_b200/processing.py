@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .scene import Scene, serialize
+from .scene import RECIPE_HY, Scene, serialize
 
 
 @dataclasses.dataclass
@@ -45,16 +45,23 @@ class EntityBuffer:
     """Serialized scene bytes on the device (processing/src/buffer.rs:13-29).
 
     `scene` is a scene.Scene (recipes HTC_RECIPE_HY / EU), already serialized bytes, or a
-    value of `scene_type` (a hypertrace_b200.types entity type, for any other scene)."""
+    value of `scene_type` (a hypertrace_b200.types entity type, for any other scene). The
+    context's config decides the layout (address width, double_support), as the reference's
+    EntityBuffer::new serializes with the context's config."""
 
     def __init__(self, context: Context, scene, scene_type=None):
+        cfg = context.config
         if isinstance(scene, (bytes, bytearray)):
             data = bytes(scene)
         elif scene_type is not None:
             from . import types as T
-            data = T.serialize(scene_type, scene, context.config.address_width)
+            data = T.serialize(scene_type, scene, cfg.address_width, cfg.double_support)
+        elif cfg.double_support:
+            from . import types as T
+            ty = T.hearth_type() if scene.recipe == RECIPE_HY else T.euclid_type()
+            data = T.serialize(ty, T.hearth_value(scene), cfg.address_width, double_support=True)
         else:
-            data = serialize(scene, context.config.address_width)
+            data = serialize(scene, cfg.address_width)
         host = torch.frombuffer(bytearray(data), dtype=torch.uint8).pin_memory()
         self.tensor = host.to(context.device, non_blocking=True)   # ordered on the current stream
         self.size = len(data)

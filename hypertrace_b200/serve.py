@@ -6,8 +6,11 @@ launch per pass, hop depth and recipe, each over every view of the step) over th
 requests, so requests that arrive while others render join the next step and their work
 overlaps on the GPU. Two classes: interactive frames (all their passes in the next step,
 admitted first) and batch jobs (a quantum of passes per step). Admission is bounded by an
-HBM budget (what does not fit waits on the host) and allocates at most a few requests per
-loop turn, so that a burst of arrivals does not hold the next step back.
+HBM budget (what does not fit waits on the host; device memory comes from a stream-ordered
+pool, so admitting never synchronises the device). The server itself -- admission,
+planning, the step's view table, read-back and release -- is native (htc_server_*,
+hypertrace_b200/csrc/htserve.cu); `Server` drives it from a Python loop of one submit per
+arrival, one step and one poll per turn.
 
 Results are bit-identical to rendering each request alone (each pixel keeps its RNG stream
 and sample order), which tests/test_gpu_serve.py checks in a mixed run.
@@ -17,17 +20,17 @@ one-pass kernel (the shape of the reference's Pipeline loop).
 """
 from __future__ import annotations
 
-import collections
+import ctypes
 import dataclasses
 import time
-from typing import Dict, List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
 
 from . import _lib
 from . import scene as S
-from .batch import BatchRenderer, View, config3
+from .batch import View, config3
 from .processing import Context, Render
 
 INTERACTIVE = 0
@@ -90,151 +93,126 @@ def make_requests(n: int, rate: float, seed: int = 0x5EED0004, interactive_share
 
 
 class Server:
-    """Continuous batching over the htc_batch launch."""
+    """Continuous batching through the native server (htc_server_*, include/htcuda.h).
+
+    The Python loop only hands arrivals to htc_server_submit, calls htc_server_step (which
+    admits by the HBM budget, plans, renders one batched step and enqueues the read-back of
+    what it completes, with up to `depth` steps in flight) and collects finished requests
+    with htc_server_poll."""
 
     def __init__(self, ctx: Context, hbm_budget_bytes: int = 120 << 30, tile_pixels: int = 512,
-                 blocks_per_sm: int = 0, gamma: float = 1.0 / 2.2, step_samples: int = 16_000_000):
+                 blocks_per_sm: int = 0, gamma: float = 1.0 / 2.2, step_samples: int = 16_000_000,
+                 depth: int = 2, admit_per_step: int = 8, max_views: int = 4096):
         self.ctx = ctx
         self.budget = hbm_budget_bytes
-        self.step_samples = step_samples    # work of one step: bounds the wait of a new arrival
-        self.renderer = BatchRenderer(ctx, max_views=4096)
-        # queues for the largest step (its views cover at most step_samples pixels, plus one
-        # oversized job), so that set_views never has to grow them mid-run
-        self.renderer.reserve(min(step_samples + 1920 * 1080, hbm_budget_bytes // 136), 8)
-        self.admit_per_step = 4             # allocations per loop turn: spreads the host work
+        self.step_samples = step_samples
         self.tile_pixels = tile_pixels
-        self.blocks_per_sm = blocks_per_sm
         self.gamma = gamma
         self.steps = 0
         self.device_s = 0.0
-        self._step_events = []
+        h = ctypes.c_void_p()
+        _lib.call("htc_server_create", hbm_budget_bytes, step_samples, max_views, ctypes.byref(h))
+        self.handle = h
+        # queues for the largest step (its views cover at most step_samples pixels, plus one
+        # oversized job), so that no step has to grow them
+        _lib.call("htc_server_configure", h, depth, tile_pixels, admit_per_step,
+                  min(step_samples + 1920 * 1080, hbm_budget_bytes // 136), ctx.stream())
 
-    def _enqueue_finish(self, r: Request, keep_image: bool) -> dict:
-        """Post chain + read-back of a finished request, enqueued on the stream (no wait)."""
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().htc_server_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def _submit(self, r: Request, keep_images: bool) -> int:
         v = r.view
+        data = v.scene.to_bytes()
         w, h = v.width, v.height
-        packed = torch.empty(w * h * 4, dtype=torch.uint8, device=self.ctx.device)
-        _lib.call("htc_extract_gamma_pack", w, h, v.spp, _lib.ctypes.c_float(self.gamma),
-                  v.canvas.image.data_ptr(), packed.data_ptr(), self.ctx.stream())
-        out = {"image": torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)}
-        out["image"].copy_(packed, non_blocking=True)
-        if keep_image:
-            out["canvas"] = torch.empty(w * h * 4, dtype=torch.float32, pin_memory=True)
-            out["canvas"].copy_(v.canvas.image, non_blocking=True)
-            out["seeds"] = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
-            out["seeds"].copy_(v.canvas.seeds, non_blocking=True)
-        v.release()   # stream-ordered reuse: the caching allocator hands the blocks out later
-        return out
+        r._scene = np.frombuffer(data, dtype=np.uint8).copy()   # type: ignore[attr-defined]
+        r._out = {"image": torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)}   # type: ignore[attr-defined]
+        if keep_images:
+            r._out["canvas"] = torch.empty(w * h * 4, dtype=torch.float32, pin_memory=True)
+            r._out["seeds"] = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
+        req = _lib.HtcRequest(r._scene.ctypes.data, len(data), w, h, v.scene.recipe, v.scene.hops, v.flags, 32,
+                              v.spp, v.global_seed & 0xFFFFFFFF,
+                              _lib.HTC_PRIORITY_INTERACTIVE if r.kind == INTERACTIVE else _lib.HTC_PRIORITY_BATCH,
+                              r.quantum, self.gamma, 0, r._out["image"].data_ptr(),
+                              r._out["canvas"].data_ptr() if keep_images else None,
+                              r._out["seeds"].data_ptr() if keep_images else None)
+        rid = ctypes.c_uint64()
+        rc = _lib.lib().htc_server_submit(self.handle, ctypes.byref(req), ctypes.byref(rid))
+        if rc == _lib.HTC_ERR_BUDGET:
+            r.refused = True
+            return 0
+        _lib.check(rc)
+        return rid.value
 
-    def _retire(self, step, t0: float, keep_images: bool) -> int:
-        event, finishing = step
-        event.synchronize()
-        t = time.perf_counter() - t0
-        for r, out in finishing:
-            r.finished = t
-            w, h = r.view.width, r.view.height
-            if keep_images:
-                r.image = out["image"].numpy().reshape(h, w, 4)
-                r.canvas = out["canvas"].numpy().reshape(h, w, 4)   # type: ignore[attr-defined]
-                r.seeds = out["seeds"].numpy().view(np.uint32).reshape(h, w)   # type: ignore[attr-defined]
-        return len(finishing)
-
-    def _plan(self, active: Sequence[Request]):
-        """Work of the next step, at most `step_samples` samples (always at least one job):
-        interactive frames first, whole, in arrival order; then batch jobs in arrival order,
-        each up to its quantum of passes, with whatever budget is left."""
-        plan, budget = [], self.step_samples
-        for r in sorted((r for r in active if r.kind == INTERACTIVE), key=lambda r: r.arrival):
-            cost = r.view.width * r.view.height * r.view.remaining
-            if cost <= budget or not plan:
-                plan.append((r, r.view.remaining))
-                budget -= cost
-        for r in sorted((r for r in active if r.kind == BATCH), key=lambda r: r.arrival):
-            px = r.view.width * r.view.height
-            p = min(r.quantum, r.view.remaining, budget // px if px else 0)
-            if p <= 0 and not plan:
-                p = 1
-            if p > 0:
-                plan.append((r, p))
-                budget -= p * px
-        return plan
-
-    def run(self, requests: Sequence[Request], keep_images: bool = False, depth: int = 2) -> Dict[str, object]:
-        """Serve `requests` in real time (arrival times relative to the call).
-
-        Steps are planned on the host from the state the already-enqueued steps will leave
-        (which requests a step finishes is known when it is enqueued), so up to `depth` steps
-        are in flight and the host's planning, admission and read-back overlap the GPU."""
+    def run(self, requests: Sequence[Request], keep_images: bool = False) -> Dict[str, object]:
+        """Serve `requests` in real time (arrival times relative to the call)."""
         arrivals = sorted(requests, key=lambda r: r.arrival)
-        ai = 0
-        waiting = collections.deque()          # arrived, not yet admitted (FIFO per class)
-        waiting_i = collections.deque()
-        active: List[Request] = []
-        inflight = collections.deque()
-        used = 0
-        t0 = time.perf_counter()
+        ai, done = 0, 0
+        by_id: Dict[int, Request] = {}
+        ids = (ctypes.c_uint64 * 256)()
+        n = ctypes.c_uint32()
+        rendered = ctypes.c_uint32()
+        info = _lib.HtcServerInfo()
         stream = torch.cuda.current_stream(self.ctx.device)
-        done = 0
+        step_events = []
+        t0 = time.perf_counter()
         while done < len(arrivals):
             now = time.perf_counter() - t0
             while ai < len(arrivals) and arrivals[ai].arrival <= now:
-                (waiting_i if arrivals[ai].kind == INTERACTIVE else waiting).append(arrivals[ai])
+                r = arrivals[ai]
                 ai += 1
-            # admission: interactive first, then batch jobs, while the HBM budget allows;
-            # a request larger than the whole budget can never run and is refused
-            admits = 0
-            for q in (waiting_i, waiting):
-                while q and q[0].view.device_bytes() > self.budget:
-                    r = q.popleft()
-                    r.refused = True
+                rid = self._submit(r, keep_images)
+                if rid:
+                    by_id[rid] = r
+                else:
                     done += 1
-                while q and admits < self.admit_per_step and used + q[0].view.device_bytes() <= self.budget:
-                    r = q.popleft()
-                    r.view.allocate(self.ctx)
-                    admits += 1
-                    r.admitted = time.perf_counter() - t0
-                    used += r.view.device_bytes()
-                    active.append(r)
-            while inflight and inflight[0][0].query():
-                done += self._retire(inflight.popleft(), t0, keep_images)
-            if not active:
-                if inflight:
-                    done += self._retire(inflight.popleft(), t0, keep_images)
-                elif ai < len(arrivals):
-                    time.sleep(max(0.0, min(arrivals[ai].arrival - now, 0.005)))
-                continue
-            if len(inflight) >= depth:
-                done += self._retire(inflight.popleft(), t0, keep_images)
-                continue
-            plan = self._plan(active)
-            self.renderer.set_views([r.view for r, _ in plan], [p for _, p in plan],
-                                    tile_pixels=self.tile_pixels, blocks_per_sm=self.blocks_per_sm)
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            self.renderer.render()
-            e1 = torch.cuda.Event(enable_timing=True)
-            e1.record(stream)
-            self._step_events.append((e0, e1))
-            self.steps += 1
-            for r, p in plan:
-                r.view.done_passes += p
-            finishing, still = [], []
-            for r in active:
-                if r.view.remaining == 0:
-                    used -= r.view.device_bytes()
-                    finishing.append((r, self._enqueue_finish(r, keep_images)))
-                else:
-                    still.append(r)
-            active = still
-            ev = torch.cuda.Event()
-            ev.record(stream)
-            inflight.append((ev, finishing))
-        while inflight:
-            done += self._retire(inflight.popleft(), t0, keep_images)
+            _lib.call("htc_server_step", self.handle, self.ctx.stream(), ctypes.byref(rendered))
+            if rendered.value:
+                e1 = torch.cuda.Event(enable_timing=True)
+                e1.record(stream)
+                step_events.append((e0, e1))
+                self.steps += 1
+            _lib.call("htc_server_poll", self.handle, ids, len(ids), ctypes.byref(n), 0)
+            t = time.perf_counter() - t0
+            for i in range(n.value):
+                r = by_id.pop(ids[i])
+                r.finished = t
+                done += 1
+                if keep_images:
+                    w, h = r.view.width, r.view.height
+                    r.image = r._out["image"].numpy().reshape(h, w, 4).copy()
+                    r.canvas = r._out["canvas"].numpy().reshape(h, w, 4).copy()   # type: ignore[attr-defined]
+                    r.seeds = r._out["seeds"].numpy().view(np.uint32).reshape(h, w).copy()   # type: ignore[attr-defined]
+                r._out = None   # type: ignore[attr-defined]
+            if not rendered.value:
+                _lib.call("htc_server_stats", self.handle, ctypes.byref(info))
+                if info.in_flight == 0 and info.active == 0 and info.waiting == 0 and ai < len(arrivals):
+                    time.sleep(max(0.0, min(arrivals[ai].arrival - (time.perf_counter() - t0), 0.005)))
+                elif info.in_flight:
+                    time.sleep(0.0002)
         torch.cuda.synchronize()
-        self.device_s = sum(a.elapsed_time(b) for a, b in self._step_events) * 1e-3
-        self.renderer.check()
+        self.device_s = sum(a.elapsed_time(b) for a, b in step_events) * 1e-3
         return summarize(arrivals, time.perf_counter() - t0, self.device_s, self.steps)
+
+    @staticmethod
+    def plan(items: Sequence[Tuple[int, int, int, int]], step_samples: int) -> List[int]:
+        """htc_serve_plan on (pixels, remaining passes, quantum, priority) items in arrival
+        order: the passes the next step gives each."""
+        arr = (_lib.HtcPlanItem * max(len(items), 1))()
+        for i, (px, rem, q, pri) in enumerate(items):
+            arr[i] = _lib.HtcPlanItem(px, rem, q, pri, 0)
+        out = (ctypes.c_uint32 * max(len(items), 1))()
+        _lib.call("htc_serve_plan", ctypes.cast(arr, ctypes.c_void_p), len(items), step_samples,
+                  ctypes.cast(out, ctypes.c_void_p))
+        return list(out)[:len(items)]
 
 
 def plain_fifo(ctx: Context, requests: Sequence[Request], gamma: float = 1.0 / 2.2) -> Dict[str, object]:

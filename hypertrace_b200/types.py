@@ -6,15 +6,18 @@ those types one for one. Each entity type knows
 
   - ``cxx()``: its C++ type expression over the templates of
     hypertrace_b200/csrc/ht_generic.cuh (what ``htc_program_build`` compiles with NVRTC),
-  - ``lay(W)``: its serialized (size, alignment) for a usize of W bytes, by the rules of
+  - ``lay(W)``: its serialized (size, alignment) for a usize of W bytes (and f64 fields of
+    ``f64_bytes(W)`` bytes: 8 when the scene is written with double_support, else 4), by the rules of
     type-macros/src/entity.rs:7-200 (fields in order, each at a multiple of its alignment;
     alignment = lcm of the fields'; size rounded up to it; an enum is a usize index with the
     payload at the enum's alignment; a Vec is a usize count with the elements at their
     alignment, types/src/containers/vector.rs:19-57),
   - ``write(buf, off, value, W)``: the bytes ``EntityBuffer::new`` uploads
-    (processing/src/buffer.rs:14-29; f64 fields as f32 when double_support is off,
-    types/src/primitive/scalar.rs:175-215; 3-vectors padded to 4 components,
-    types/src/primitive/vector.rs:74-106).
+    (processing/src/buffer.rs:14-29; f64 fields as f32 when double_support is off, as f64
+    when it is on, types/src/primitive/scalar.rs:175-215; 3-vectors padded to 4 components,
+    types/src/primitive/vector.rs:74-106; a primitive vector or matrix is aligned to its own
+    size, types/src/primitive/matrix.rs:171-209). Colors and the gradient power are f32 in
+    the reference and stay 4 bytes either way.
 
 Values are plain Python data: floats, 3-/4-sequences, 2x2 complex arrays (Moebius),
 ``(outer, inner)`` tuples (Chain), dicts keyed by field name (structs), ``(variant index,
@@ -42,6 +45,25 @@ def lcm(a: int, b: int) -> int:
 
 def _usize_bytes(x: int, W: int) -> bytes:
     return struct.pack("<I" if W == 4 else "<Q", int(x))
+
+
+class Cfg(int):
+    """The layout parameter every entity method takes: an int (the usize size in bytes, 4 or
+    8) that also carries the size of an f64 field (4, or 8 with double_support)."""
+
+    def __new__(cls, usize: int, f64: int = 4):
+        obj = super().__new__(cls, usize)
+        obj.f64 = f64
+        return obj
+
+
+def f64_bytes(W) -> int:
+    """Bytes of an f64 field under layout parameter W (a plain int means double_support off)."""
+    return getattr(W, "f64", 4)
+
+
+def _pack_reals(buf, off, W, values) -> None:
+    struct.pack_into("<%d%s" % (len(values), "d" if f64_bytes(W) == 8 else "f"), buf, off, *[float(v) for v in values])
 
 
 class Entity:
@@ -83,6 +105,8 @@ class Unit(Entity):
 
 
 class F32(Entity):
+    """An f32 field (the gradient background's power)."""
+
     def cxx(self):
         return "F32"
 
@@ -93,8 +117,22 @@ class F32(Entity):
         struct.pack_into("<f", buf, off, float(value))
 
 
+class F64(Entity):
+    """An f64 field (fov, portions, refractive index, tiling sizes): 4 bytes as f32, or 8."""
+
+    def cxx(self):
+        return "F32"
+
+    def lay(self, W):
+        f = f64_bytes(W)
+        return (f, f)
+
+    def write(self, buf, off, value, W):
+        _pack_reals(buf, off, W, [value])
+
+
 class Vec3(Entity):
-    """Vector<f32 | f64, 3>: 16 bytes, aligned to 16."""
+    """Vector<f32, 3> (colors): 16 bytes, aligned to 16."""
 
     def cxx(self):
         return "R3"
@@ -107,16 +145,32 @@ class Vec3(Entity):
         struct.pack_into("<fff", buf, off, v[0], v[1], v[2])
 
 
+class Vec3F64(Entity):
+    """Vector<f64, 3> (directions, shifts): 4 reals, aligned to their size."""
+
+    def cxx(self):
+        return "R3"
+
+    def lay(self, W):
+        f = f64_bytes(W)
+        return (4 * f, 4 * f)
+
+    def write(self, buf, off, value, W):
+        _pack_reals(buf, off, W, [float(x) for x in value][:3])
+
+
 class Quat(Entity):
+    """Quaternion<f64> (rotations): 4 reals, aligned to their size."""
+
     def cxx(self):
         return "Quat"
 
     def lay(self, W):
-        return (16, 16)
+        f = f64_bytes(W)
+        return (4 * f, 4 * f)
 
     def write(self, buf, off, value, W):
-        v = [float(x) for x in value]
-        struct.pack_into("<ffff", buf, off, *v)
+        _pack_reals(buf, off, W, [float(x) for x in value])
 
 
 class Array(Entity):
@@ -268,12 +322,13 @@ class Moebius(Entity):
         return "Moebius"
 
     def lay(self, W):
-        return (32, 32)
+        f = f64_bytes(W)
+        return (8 * f, 8 * f)
 
     def write(self, buf, off, value, W):
         m = np.asarray(value, dtype=np.complex128)
         vals = [m[0, 0], m[0, 1], m[1, 0], m[1, 1]]
-        struct.pack_into("<8f", buf, off, *[float(x) for z in vals for x in (z.real, z.imag)])
+        _pack_reals(buf, off, W, [float(x) for z in vals for x in (z.real, z.imag)])
 
 
 class Shift3(Entity):
@@ -283,10 +338,10 @@ class Shift3(Entity):
         return "Shift3"
 
     def lay(self, W):
-        return (16, 16)
+        return Vec3F64().lay(W)
 
     def write(self, buf, off, value, W):
-        Vec3().write(buf, off, value, W)
+        Vec3F64().write(buf, off, value, W)
 
 
 class Rotation3(Entity):
@@ -297,7 +352,7 @@ class Rotation3(Entity):
         return "Rotation3"
 
     def lay(self, W):
-        return (16, 16)
+        return Quat().lay(W)
 
     def write(self, buf, off, value, W):
         Quat().write(buf, off, value, W)
@@ -312,13 +367,14 @@ class Linear3(Entity):
         return "Linear3"
 
     def lay(self, W):
-        return (64, 64)
+        f = f64_bytes(W)
+        return (16 * f, 16 * f)
 
     def write(self, buf, off, value, W):
         m = np.asarray(value, dtype=np.float64).reshape(3, 3)
         vals = [float(m[i, j]) for i in range(3) for j in range(3)]
         flat = vals[0:3] + [0.0] + vals[3:6] + [0.0] + vals[6:9] + [0.0] + [0.0, 0.0, 0.0, 1.0]
-        struct.pack_into("<16f", buf, off, *flat)
+        _pack_reals(buf, off, W, flat)
 
 
 class Chain(Entity):
@@ -351,7 +407,7 @@ def Homogenous3() -> Chain:
 
 def PointView(geo: str) -> Struct:
     """PointView<G>{fov, phantom} (objects/src/view/point.rs:11-14); value: {"fov": f}."""
-    return Struct(f"PointView<{geo}>", [("fov", F32()), ("phantom", Unit())])
+    return Struct(f"PointView<{geo}>", [("fov", F64()), ("phantom", Unit())])
 
 
 def MappedView(geo: str, view: Entity, map_: Entity) -> Struct:
@@ -416,7 +472,7 @@ def Transparent() -> Unit:
 
 def Refractive() -> Struct:
     """{index} (objects/src/material/refractive.rs)."""
-    return Struct("Refractive", [("index", F32())])
+    return Struct("Refractive", [("index", F64())])
 
 
 def Colored(inner: Entity) -> Struct:
@@ -431,7 +487,7 @@ def Emissive(inner: Entity) -> Struct:
 
 def Component(material: Entity) -> Struct:
     """{material, portion} (objects/src/material/mixture.rs:4-9)."""
-    return Struct(f"Component<{material.cxx()}>", [("material", material), ("portion", F32())])
+    return Struct(f"Component<{material.cxx()}>", [("material", material), ("portion", F64())])
 
 
 def Mixture(*components: Tuple[str, Entity]) -> Struct:
@@ -469,7 +525,7 @@ _HORO_TILINGS = {"Uniform": "HoroUniform", "Square": "HoroSquare", "Hexagonal": 
 def _tiled(kind: str, material: Entity, tiling: str, n: int) -> Struct:
     return Struct(f"{kind}<{material.cxx()}, {tiling}, {n}>",
                   [("tiling", Unit()), ("materials", Array(material, n)), ("border_material", material),
-                   ("cell_size", F32()), ("border_width", F32())])
+                   ("cell_size", F64()), ("border_width", F64())])
 
 
 def TiledPlane(material: Entity, tiling: str, n: int) -> Struct:
@@ -492,7 +548,7 @@ def ConstBg() -> Struct:
 
 def GradBg() -> Struct:
     """{direction, colors[2], power} (objects/src/background/basic.rs:54-58)."""
-    return Struct("GradBg", [("direction", Vec3()), ("colors", Array(Vec3(), 2)), ("power", F32())])
+    return Struct("GradBg", [("direction", Vec3F64()), ("colors", Array(Vec3(), 2)), ("power", F32())])
 
 
 # ----------------------------------------------------------------------------- scene
@@ -504,18 +560,23 @@ def SceneImpl(geo: str, view: Entity, obj: Entity, background: Entity) -> Struct
                   [("geometry", Unit()), ("view", view), ("background", background), ("object", obj)])
 
 
-def serialize(scene_type: Entity, value, address_width: int = 32) -> bytes:
-    W = 4 if address_width == 32 else 8
+def layout(address_width: int = 32, double_support: bool = False) -> Cfg:
+    """The layout parameter of a types::Config (types/src/config.rs:38-43)."""
     if address_width not in (32, 64):
         raise ValueError("address_width must be 32 or 64")
+    return Cfg(4 if address_width == 32 else 8, 8 if double_support else 4)
+
+
+def serialize(scene_type: Entity, value, address_width: int = 32, double_support: bool = False) -> bytes:
+    W = layout(address_width, double_support)
     buf = bytearray(scene_type.size_of(value, W))
     scene_type.write(buf, 0, value, W)
     return bytes(buf)
 
 
-def static_size(scene_type: Entity, address_width: int = 32) -> int:
+def static_size(scene_type: Entity, address_width: int = 32, double_support: bool = False) -> int:
     """Bytes of the scene without its dynamic part (htc_program_static_size)."""
-    W = 4 if address_width == 32 else 8
+    W = layout(address_width, double_support)
     if isinstance(scene_type, Struct) and scene_type.dynamic:
         offs = scene_type.offsets(W)
         return offs[-1] + scene_type.fields[-1][1].lay(W)[0]

@@ -25,6 +25,7 @@ extern "C" {
 #define HTC_ERR_CUDA (-2)         /* a CUDA runtime call failed */
 #define HTC_ERR_SCENE (-3)        /* scene bytes failed validation (device-side check) */
 #define HTC_ERR_UNSUPPORTED (-4)  /* configuration this build does not serve */
+#define HTC_ERR_BUDGET (-5)       /* a request needs more device memory than the server's whole budget */
 
 /* ---------------------------------------------------------------- scene recipes
  * The scene types the hand-written kernels serve (the Rust types that the reference's
@@ -208,6 +209,79 @@ int htc_batch_render(htc_batch *batch, uint64_t *stats, void *stream);
 int htc_batch_graph_launch(htc_batch *batch, uint64_t *stats, void *stream);
 /* Reads and clears the batch's device error word (synchronises `stream`). */
 int htc_batch_check(htc_batch *batch, void *stream);
+
+/* ---------------------------------------------------------------- serving
+ * A continuous-batching render server (no counterpart in the reference, whose examples render
+ * one view per frame in a time-budgeted loop, main/examples/hearth.rs:116-135). Requests are
+ * submitted at any time; every htc_server_step admits waiting requests while their device
+ * memory fits the HBM budget (interactive ones first; memory from a stream-ordered pool, so
+ * admission never synchronises the device), plans the step (htc_serve_plan) and renders the
+ * planned passes of all admitted requests together (the batch launches above). Requests that
+ * a step completes get the post chain and their read-back enqueued after it, and their device
+ * memory released; htc_server_poll reports them once their host buffers are written. Each
+ * request's result is bit-identical to rendering it alone. One server serves one stream and
+ * one host thread at a time. */
+#define HTC_PRIORITY_INTERACTIVE 0   /* all remaining passes in the next step, planned first */
+#define HTC_PRIORITY_BATCH 1         /* up to `quantum` passes per step, with what is left */
+
+typedef struct htc_request {
+    const void *scene;       /* host pointer to the serialized scene bytes (copied at submission) */
+    uint64_t scene_size;
+    uint32_t width, height;
+    int32_t recipe;          /* HTC_RECIPE_HY or HTC_RECIPE_EU */
+    uint32_t light_hops;
+    uint32_t flags;          /* HTC_FLAG_* */
+    int32_t address_width;   /* 32 or 64 */
+    uint32_t passes;         /* samples per pixel to render */
+    uint32_t global_seed;    /* per-pixel seeds as htc_fill_seeds(seeds, w*h, global_seed, 0) */
+    uint32_t priority;       /* HTC_PRIORITY_* */
+    uint32_t quantum;        /* batch jobs: passes per step */
+    float gamma;             /* post chain exponent (1/2.2 in the reference's pipeline) */
+    uint32_t reserved;
+    void *out_rgba8;         /* host, width*height*4 bytes: the packed image (pinned keeps the copy async) */
+    void *out_canvas;        /* host, width*height*16 bytes, or NULL: the float4 accumulation */
+    void *out_seeds;         /* host, width*height*4 bytes, or NULL: the final RNG states */
+} htc_request;
+
+/* One request as the planner sees it. */
+typedef struct htc_plan_item {
+    uint64_t pixels;
+    uint32_t remaining;      /* passes still to render */
+    uint32_t quantum;
+    uint32_t priority;
+    uint32_t reserved;
+} htc_plan_item;
+
+typedef struct htc_server_info {
+    uint32_t waiting, active, in_flight, finished;
+    uint64_t used_bytes, budget_bytes, steps;
+} htc_server_info;
+
+typedef struct htc_server htc_server;
+/* The step planner alone (host only, no device): passes[i] for items in arrival order --
+ * interactive items whole while they fit `step_samples` samples (the first one always), then
+ * batch items up to their quantum with what is left (at least one pass when nothing else runs). */
+int htc_serve_plan(const htc_plan_item *items, uint32_t n, uint64_t step_samples, uint32_t *passes);
+/* A server for the current device: `hbm_budget` bytes of request memory (scene, canvas, seeds,
+ * image and a 136-byte-per-pixel share of the wavefront queues), steps of at most
+ * `step_samples` samples (bounds how long a new arrival waits), up to `max_views` requests in
+ * one step. */
+int htc_server_create(uint64_t hbm_budget, uint64_t step_samples, uint32_t max_views, htc_server **out);
+void htc_server_destroy(htc_server *server);
+/* Steps in flight (default 2), the batch tile size (default 512), admissions per step
+ * (default 8), and queue slots to reserve up front (0 = none). */
+int htc_server_configure(htc_server *server, uint32_t depth, uint32_t tile_pixels, uint32_t admit_per_step,
+                         uint64_t reserve_pixels, void *stream);
+/* Queues a request (copies its scene bytes); *id identifies it in htc_server_poll.
+ * HTC_ERR_BUDGET when it alone needs more than the whole budget. */
+int htc_server_submit(htc_server *server, const htc_request *request, uint64_t *id);
+/* One step on `stream` (see above); *rendered_views (may be NULL) = requests it renders
+ * (0 when nothing is admitted). Blocks only while `depth` steps are still in flight. */
+int htc_server_step(htc_server *server, void *stream, uint32_t *rendered_views);
+/* Ids of finished requests (host buffers written), up to max_ids; wait_all != 0 first waits
+ * for every step in flight. */
+int htc_server_poll(htc_server *server, uint64_t *ids, uint32_t max_ids, uint32_t *n, int wait_all);
+int htc_server_stats(const htc_server *server, htc_server_info *info);
 
 /* ---------------------------------------------------------------- post chain
  * Extractor (processing/src/canvas.rs:126-135): image = canvas / passes.

@@ -1,7 +1,9 @@
 /* cull_check.c -- test infrastructure: a CPU restatement of the distance-bound culling of the
  * hyperbolic object scan (hypertrace_b200/csrc/ht_trace.cuh: stage_bound, bound_ray,
- * culled_point, culled_fw, sure_crossing_e2, upper_estimate, cull_from_dist and the chunked
- * scan of hop_hy), run against the full scan on every hop of sampled paths.
+ * point_cut / survivors2 / culled_slot, culled_fw, sure_crossing_e2, upper_estimate,
+ * cull_from_dist and the chunked scan of hop_hy over the staged slots: planes first, then
+ * horospheres, each in scene order, hits compared on (distance, scene index)), run against
+ * the full scan on every hop of sampled paths.
  *
  * The culling may only skip objects that cannot win, so on every hop the culled scan must pick
  * the object the full scan picks (the nearest reported hit, ties to the lowest index) at the
@@ -88,12 +90,15 @@ static cull_t cull_from_dist(float d) {
     return c;
 }
 static cull_t cull_none(void) { cull_t c = {INFINITY, INFINITY, 1.0f}; return c; }
+/* point bound of one slot: culled when F + eF < lo or F - eF > hi (point_cut / survivors2) */
 static int culled_point(f4 rec, float mag, uint32_t shape, const bray_t *r, cull_t c) {
     float t = r->t;
     float F = fmaf(rec.x, r->r2, fmaf(rec.y, r->x, fmaf(rec.z, r->y, rec.w)));
     float eF = mag * r->K;
-    if (shape == 0) return fabsf(F) - eF > 2.0f * t * c.S;
-    return t > c.E * (F + eF) || t * c.E < F - eF;
+    float lo, hi;
+    if (shape == 0) { hi = 2.0f * t * c.S; lo = -hi; }
+    else { lo = t * adv(1.0f / c.E, +1); hi = t * c.E; }
+    return (F + eF < lo) || (F + (mag * -r->K) > hi);
 }
 static fw_t bound_fw(f4 rec, float mag, const bray_t *r) {
     fw_t b;
@@ -164,10 +169,15 @@ static float dist_from_e2(float x) { return 0.5f * LN2F * (float)log2((double)x)
 
 typedef struct { f4 *bound; float *mag; uint32_t *shape; } staged_t;
 
-static float upper_estimate(const staged_t *st, uint32_t n, const bray_t *r, uint32_t prev) {
+/* over the first EST_OBJECTS / 2 planes and the first EST_OBJECTS / 2 horospheres */
+static float upper_estimate(const staged_t *st, const uint32_t *slot_obj, uint32_t n, uint32_t np, const bray_t *r,
+                            uint32_t prev) {
     float best = INFINITY;
-    for (uint32_t k = 0; k < n; ++k)
-        best = fminf(best, sure_crossing_e2(bound_fw(st->bound[k], st->mag[k], r), st->shape[k], k == prev, r->t));
+    const uint32_t half = EST_OBJECTS / 2;
+    for (uint32_t q = 0; q < n; ++q) {
+        if (!(q < np ? q < half : q - np < half)) continue;
+        best = fminf(best, sure_crossing_e2(bound_fw(st->bound[q], st->mag[q], r), st->shape[q], slot_obj[q] == prev, r->t));
+    }
     return best < INFINITY ? dist_from_e2(best) : best;
 }
 
@@ -197,6 +207,23 @@ int main(int argc, char **argv) {
         st.mag[k] = bound_mag(st.bound[k]);
     }
     long long n_hops = 0, n_exact = 0, wrong = 0;
+    /* scan order of the staged slots: planes, then horospheres, each in scene order (the
+     * kernel's dummy slot after an odd number of planes is never a candidate: left out) */
+    uint32_t *slot_obj = malloc(sizeof(uint32_t) * (sc.n + 1));
+    uint32_t ns = 0, np = 0;
+    for (uint32_t k = 0; k < sc.n; ++k) np += st.shape[k] == 0;
+    for (uint32_t want = 0; want < 2; ++want)
+        for (uint32_t k = 0; k < sc.n; ++k)
+            if (st.shape[k] == want) slot_obj[ns++] = k;
+    staged_t ss;
+    ss.bound = malloc(sizeof(f4) * (sc.n + 1));
+    ss.mag = malloc(sizeof(float) * (sc.n + 1));
+    ss.shape = malloc(sizeof(uint32_t) * (sc.n + 1));
+    for (uint32_t q = 0; q < sc.n; ++q) {
+        ss.bound[q] = st.bound[slot_obj[q]];
+        ss.mag[q] = st.mag[slot_obj[q]];
+        ss.shape[q] = st.shape[slot_obj[q]];
+    }
     for (uint32_t pi = 0; pi < npix; ++pi) {
         uint32_t px = (uint32_t)(((uint64_t)pi * 2654435761u) % ((uint64_t)W * H));
         uint32_t rng = fmix32(gseed ^ fmix32(px));
@@ -227,29 +254,30 @@ int main(int argc, char **argv) {
             int can = cull_point_ok(ray.start);
             cull_t cull = cull_none();
             if (can) {
-                float u = upper_estimate(&st, sc.n < EST_OBJECTS ? sc.n : EST_OBJECTS, &br, prev);
+                float u = upper_estimate(&ss, slot_obj, sc.n, np, &br, prev);
                 if (u < INFINITY) cull = cull_from_dist(u);
             }
             R cd = -1; uint32_t ck = 0;
             for (uint32_t c0 = 0; c0 < sc.n; c0 += 32) {
                 uint32_t cn = sc.n - c0 < 32 ? sc.n - c0 : 32, mask = 0;
                 for (uint32_t j = 0; j < cn; ++j)
-                    if (!can || !culled_point(st.bound[c0 + j], st.mag[c0 + j], st.shape[c0 + j], &br, cull)) mask |= 1u << j;
+                    if (!can || !culled_point(ss.bound[c0 + j], ss.mag[c0 + j], ss.shape[c0 + j], &br, cull)) mask |= 1u << j;
                 if (can)
                     for (uint32_t j = 0; j < cn; ++j)
-                        if ((mask >> j & 1) && culled_fw(bound_fw(st.bound[c0 + j], st.mag[c0 + j], &br), st.shape[c0 + j], br.t, cull))
+                        if ((mask >> j & 1) && culled_fw(bound_fw(ss.bound[c0 + j], ss.mag[c0 + j], &br), ss.shape[c0 + j], br.t, cull))
                             mask &= ~(1u << j);
                 for (uint32_t j = 0; j < cn; ++j) {
                     if (!(mask >> j & 1)) continue;
-                    uint32_t k = c0 + j;
-                    if (can && culled_point(st.bound[k], st.mag[k], st.shape[k], &br, cull)) continue;
+                    uint32_t q = c0 + j, k = slot_obj[q];
+                    if (can && culled_point(ss.bound[q], ss.mag[q], ss.shape[q], &br, cull)) continue;
                     int rep = (k == prev);
-                    if (st.shape[k] == 0 && rep) continue;
+                    if (ss.shape[q] == 0 && rep) continue;
                     ++n_exact;
                     ray_hy local = ray_hy_map(ray, sc.mo_inv[k]);
                     quat nrm;
-                    R d = st.shape[k] == 0 ? plane_hy_detect(rep, &nrm, &local) : horosphere_detect(rep, &nrm, &local);
-                    if (d > -EPS && (cd <= -EPS || d < cd)) { cd = d; ck = k; cull = cull_from_dist((float)d); }
+                    R d = ss.shape[q] == 0 ? plane_hy_detect(rep, &nrm, &local) : horosphere_detect(rep, &nrm, &local);
+                    /* (distance, scene index): the slots are not in scene order */
+                    if (d > -EPS && (cd <= -EPS || d < cd || (d == cd && k < ck))) { cd = d; ck = k; cull = cull_from_dist((float)d); }
                 }
             }
             if ((cd > -EPS) != (min_dist > -EPS) || (cd > -EPS && (cd != min_dist || ck != min_index))) ++wrong;

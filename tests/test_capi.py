@@ -40,8 +40,9 @@ def test_errors_without_device(built):
     assert b"recipe" in _lib.lib().htc_last_error()
     rc = _lib.lib().htc_program_create(1, 0, 32, 0, 0, ctypes.byref(h))
     assert rc == _lib.HTC_ERR_INVALID
-    rc = _lib.lib().htc_program_create(1, 4, 32, 1, 0, ctypes.byref(h))
+    rc = _lib.lib().htc_program_create(3, 4, 32, 1, 0, ctypes.byref(h))   # double_support: HY / EU recipes only
     assert rc == _lib.HTC_ERR_UNSUPPORTED
+    assert b"double_support" in _lib.lib().htc_last_error()
     rc = _lib.lib().htc_render(None, 4, 4, None, 0, None, None, None)
     assert rc == _lib.HTC_ERR_INVALID
 

@@ -232,6 +232,43 @@ def test_pack_bytes_equal_oracle(built):
     assert bad.size == 0, f"{bad.size} pixels differ, first {img[bad[:4]]} -> {got[bad[:4]]} vs {want[bad[:4]]}"
 
 
+@pytest.mark.parametrize("cfg", ["config1", "config0"])
+def test_double_support_scene_renders_as_its_f32_serialization(built, cfg):
+    """A scene serialized with double_support (8-byte f64 fields, f64 vectors and maps aligned
+    to their size) is narrowed on the device to the f32 layout, each f64 rounded to the
+    nearest f32 -- what the reference serializes without double_support -- and renders bit
+    for bit as the f32 serialization does (one-pass kernel and htc_render_passes)."""
+    wl = getattr(S, cfg)()
+    W, H = 96, 64
+    out = []
+    for double in (False, True):
+        ctx = P.Context(0, P.Config(double_support=double))
+        buf = P.EntityBuffer(ctx, wl.scene)
+        r = P.Render(ctx, wl.scene.recipe, wl.scene.hops)
+        a = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
+        r.render(buf, a)
+        r.render_passes(buf, a, 3)
+        torch.cuda.synchronize()
+        out.append((buf.size, r.static_size(), a.image.cpu().numpy().view(np.uint32).copy(), a.seeds.cpu().numpy().copy()))
+    (fsize, fstatic, fimg, fseeds), (dsize, dstatic, dimg, dseeds) = out
+    assert dsize > fsize and dstatic > fstatic   # the double layout is larger
+    assert np.array_equal(fseeds, dseeds)
+    assert np.array_equal(fimg, dimg)
+
+
+def test_double_support_bad_object_count_is_reported(built):
+    wl = S.config1()
+    ctx = P.Context(0, P.Config(double_support=True))
+    buf = P.EntityBuffer(ctx, wl.scene)
+    data = bytearray(buf.tensor.cpu().numpy().tobytes())
+    data[192:196] = (10_000).to_bytes(4, "little")   # object count of the double layout
+    buf.tensor.copy_(torch.frombuffer(data, dtype=torch.uint8).to(ctx.device))
+    r = P.Render(ctx, wl.scene.recipe, wl.scene.hops)
+    with pytest.raises(_lib.HtcError) as e:
+        r.render(buf, P.Canvas(ctx, (16, 16)))
+    assert e.value.code == _lib.HTC_ERR_SCENE
+
+
 def test_invalid_scene_is_reported(built):
     ctx = P.Context(0)
     wl = S.config1()

@@ -46,6 +46,24 @@ def test_served_equals_alone(built, budget):
         assert served.finished >= served.arrival
 
 
+def test_oversized_request_is_refused_and_memory_returns(built):
+    """A request needing more device memory than the whole budget is refused at submission
+    (HTC_ERR_BUDGET); the others are served and the budget's bytes all come back."""
+    from hypertrace_b200 import _lib
+    import ctypes
+    ctx = P.Context(0)
+    reqs = _requests(n=5)
+    sc = S.hyperbolic_scene(3, 3, 5.0, 8, 1)
+    reqs.append(V.Request(99, V.INTERACTIVE, 0.0, B.View(sc, 1280, 720, 8, 7)))   # 1280x720 x 160 B > 2 MB
+    srv = V.Server(ctx, hbm_budget_bytes=2_000_000, tile_pixels=512)
+    res = srv.run(reqs)
+    assert res["refused"] == 1 and res["requests"] == 5
+    assert next(r for r in reqs if r.rid == 99).refused
+    info = _lib.HtcServerInfo()
+    _lib.call("htc_server_stats", srv.handle, ctypes.byref(info))
+    assert info.used_bytes == 0 and info.active == 0 and info.waiting == 0 and info.in_flight == 0
+
+
 def test_plain_fifo_runs(built):
     ctx = P.Context(0)
     reqs = _requests(n=4)
