@@ -18,7 +18,8 @@ SRCS = [os.path.join(HERE, "csrc", "htcuda.cu"), os.path.join(HERE, "csrc", "htg
         os.path.join(HERE, "csrc", "htserve.cu")]
 OUT = os.path.join(HERE, "libhtcuda.so")
 # Device headers that htc_program_build hands to NVRTC, embedded as C strings.
-NVRTC_HEADERS = [("k_header_ht_math", "ht_math.cuh"), ("k_header_ht_generic", "ht_generic.cuh")]
+NVRTC_HEADERS = [("k_header_ht_math", "ht_math.cuh"), ("k_header_ht_bound", "ht_bound.cuh"),
+                 ("k_header_ht_generic", "ht_generic.cuh")]
 GENERATED = os.path.join(HERE, "csrc", "generated", "nvrtc_headers.inc")
 
 NVCC_FLAGS = [

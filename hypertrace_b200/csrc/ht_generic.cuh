@@ -33,6 +33,7 @@
 //   scene       SceneImpl<G, V, O, B> (render/scene.inl; the hop count H is a launch argument)
 #pragma once
 #include "ht_math.cuh"
+#include "ht_bound.cuh"
 
 namespace htg {
 using namespace ht;
@@ -138,6 +139,14 @@ struct Ctx {
     u32 tests;      // leaf object tests (statistics)
     Ptr end;        // one past the scene bytes: dynamic containers are clamped to it
     u32 *err;
+    // distance bounds of the scene's top-level object vector, staged in shared memory by the
+    // kernel (render_generic): bvec is that vector's address (NULL: no culling), culled counts
+    // the element tests the bounds skipped (statistics)
+    Ptr bvec;
+    const float4 *brec;
+    const float *bmag;
+    const u32 *bkind;
+    u32 culled;
 };
 HT_D bool is_repeat(const Ctx &c) { return c.hasher == c.prev; }
 HT_D void hash_usize(Ctx &c, u32 x) { const u32 h = c.hasher; c.hasher = x + (h << 6) + (h << 16) - h; }
@@ -717,7 +726,9 @@ template <class G, class O> struct ObjectVec {   // object/vector.inl
         if (stride > 0 && (c.end < self + head || n > (u32)((c.end - self - head) / stride))) { atomicOr(c.err, ERR_SCENE); n = 0; }
         return n;
     }
-    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    template <int W, bool F = true> HT_D static float detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l);
+    template <int W, bool F> HT_D static float detect_culled(Ptr self, Ctx &c, Cache &cache, Light<G> &l);
+    template <int W, bool F = true> HT_D static float detect_all(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
         constexpr u32 stride = O::template lay<W>().size;
         constexpr u32 head = upm((u32)W, O::template lay<W>().align);
         // Distances first (no map back, no hit direction), then the winner's full detection
@@ -1007,9 +1018,173 @@ template <class M, class K, int N> struct TiledHorosphere {   // object/hy/tiled
     }
 };
 
+// ============================================================================ distance bounds
+// Which hyperbolic shape an object is, for the world-space distance bounds of ht_bound.cuh:
+// kind 0 = geodesic plane, 1 = horosphere, 2 = read from the object's bytes (a choice whose
+// variants are all plane- or horosphere-shaped), -1 = none (the object is never culled).
+// of<W>(self) gives the shape of one object (2 for kind -1: no bound record).
+template <class O> struct BoundKind {
+    static constexpr int kind = -1;
+    template <int W> HT_D static u32 of(Ptr) { return 2u; }
+};
+template <int K> struct BoundKindFixed {
+    static constexpr int kind = K;
+    template <int W> HT_D static u32 of(Ptr) { return (u32)K; }
+};
+template <> struct BoundKind<PlaneHy> : BoundKindFixed<0> {};
+template <> struct BoundKind<Horosphere> : BoundKindFixed<1> {};
+template <class M, class K, int N> struct BoundKind<TiledPlane<M, K, N>> : BoundKindFixed<0> {};
+template <class M, class K, int N> struct BoundKind<TiledHorosphere<M, K, N>> : BoundKindFixed<1> {};
+template <class S, class M> struct BoundKind<Covered<Hy, S, M>> {
+    static constexpr int kind = BoundKind<S>::kind;
+    template <int W> HT_D static u32 of(Ptr self) { return BoundKind<S>::template of<W>(self + Rec<W, Zst, M, S>::off(2)); }
+};
+// A choice: the shape of the variant its index names (all variants of a fixed kind).
+template <class... V> struct VariantKind;
+template <> struct VariantKind<> {
+    static constexpr bool fixed = true;
+    HT_D static u32 of(u32) { return 2u; }
+};
+template <class V0, class... V> struct VariantKind<V0, V...> {
+    static constexpr bool fixed = (BoundKind<V0>::kind == 0 || BoundKind<V0>::kind == 1) && VariantKind<V...>::fixed;
+    HT_D static u32 of(u32 i) { return i == 0 ? (u32)BoundKind<V0>::kind : VariantKind<V...>::of(i - 1); }
+};
+template <class... S> struct BoundKind<ShapeChoice<Hy, S...>> {
+    static constexpr int kind = VariantKind<S...>::fixed ? 2 : -1;
+    template <int W> HT_D static u32 of(Ptr self) { return kind == 2 ? VariantKind<S...>::of(ldusize<W>(self)) : 2u; }
+};
+template <class... O> struct BoundKind<ObjectChoice<Hy, O...>> {
+    static constexpr int kind = VariantKind<O...>::fixed ? 2 : -1;
+    template <int W> HT_D static u32 of(Ptr self) { return kind == 2 ? VariantKind<O...>::of(ldusize<W>(self)) : 2u; }
+};
+
+// A vector of Moebius-mapped objects of a known shape gets distance bounds: one world-space
+// record per element (stage_bound of the element's map) in shared memory, staged once per
+// block by render_generic when the vector is the scene's top-level object and holds at most
+// HTG_BOUND_CAP elements.
+#ifndef HTG_BOUND_CAP
+#define HTG_BOUND_CAP 256u
+#endif
+template <class G, class O> struct VecBounds { static constexpr bool ok = false; };
+template <class X> struct VecBounds<Hy, MappedObject<Hy, X, Moebius>> {
+    static constexpr bool ok = BoundKind<X>::kind >= 0;
+    template <int W> HT_D static u32 kind_of(Ptr elem) {
+        return BoundKind<X>::template of<W>(elem + Rec<W, Zst, Moebius, X>::off(2));
+    }
+    template <int W> HT_D static Mo map_of(Ptr elem) { return Moebius::load(elem + Rec<W, Zst, Moebius, X>::off(1)); }
+};
+// Stages the records of the vector at `self` (all threads of the block; returns the element
+// count staged, or 0xFFFFFFFF when the vector is too large or its count does not fit the bytes).
+template <class G, class O, int W>
+HT_D u32 stage_vec_bounds(Ptr self, Ptr end, float4 *rec, float *mag, u32 *kind) {
+    typedef VecBounds<G, O> B;
+    constexpr u32 stride = O::template lay<W>().size;
+    constexpr u32 head = upm((u32)W, O::template lay<W>().align);
+    const u32 n = ldusize<W>(self);
+    if (stride == 0 || end < self + head || n > (u32)((end - self - head) / stride) || n > HTG_BOUND_CAP) return 0xFFFFFFFFu;
+    const float nan = __int_as_float(0x7fc00000);
+    for (u32 i = threadIdx.x; i < n; i += blockDim.x) {
+        const Ptr elem = self + head + i * stride;
+        const u32 k = B::template kind_of<W>(elem);
+        const float4 r = k <= 1u ? stage_bound(B::template map_of<W>(elem), k) : make_float4(nan, nan, nan, nan);
+        rec[i] = r;
+        mag[i] = bound_mag(r);
+        kind[i] = k;
+    }
+    return n;
+}
+
+template <class G, class O> template <int W, bool F>
+HT_D float ObjectVec<G, O>::detect(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    if constexpr (VecBounds<G, O>::ok) {
+        if (c.bvec == self) return detect_culled<W, F>(self, c, cache, l);
+    }
+    return detect_all<W, F>(self, c, cache, l);
+}
+
+// The scan of ObjectVec::detect_all with the distance bounds of the hand-written hyperbolic
+// kernel (ht_trace.cuh hop_hy): an upper estimate of the nearest sure crossing among the first
+// 32 elements sets a threshold before the first exact test, each chunk of 32 elements is
+// culled by the point bound (warp-uniform) and the ray-aware bound (per lane), and the
+// survivors are tested in index order with the threshold tightening on every nearer hit. The
+// elements are visited in index order, so the reference's comparison (object/vector.inl:37-50)
+// is unchanged; culling only skips elements that cannot be nearer than the threshold.
+template <class G, class O> template <int W, bool F>
+HT_D float ObjectVec<G, O>::detect_culled(Ptr self, Ctx &c, Cache &cache, Light<G> &l) {
+    constexpr u32 stride = O::template lay<W>().size;
+    constexpr u32 head = upm((u32)W, O::template lay<W>().align);
+    const u32 n = count<W>(self, c);
+    const u32 orig = c.hasher;
+    const Q4 p = l.p, v = l.v;
+    const bool can = cull_point_ok(p);
+    const BoundRay br = bound_ray(p, v);
+    Cull cull = cull_none();
+    if (can) {
+        float best = __int_as_float(0x7f800000);
+        const u32 ne = n < 32u ? n : 32u;
+        for (u32 i = 0; i < ne; ++i) {   // warp-uniform: broadcast loads
+            const u32 h = i + (orig << 6) + (orig << 16) - orig;   // the element's hash (hash_usize)
+            best = fminf(best, sure_crossing_e2(bound_fw(c.brec[i], c.bmag[i], br), c.bkind[i], h == c.prev, br.t));
+        }
+        if (best < __int_as_float(0x7f800000)) cull = cull_from_dist(dist_from_e2(best));
+    }
+    PointCut kp = point_cut(0, br.t, cull), kh = point_cut(1, br.t, cull);
+    float min_dist = -1.0f;
+    u32 min_index = 0, min_hasher = orig, tested = 0;
+    for (u32 c0 = 0; c0 < n; c0 += 32) {
+        const u32 cn = n - c0 < 32u ? n - c0 : 32u;
+        u32 mask = cn == 32u ? 0xFFFFFFFFu : (1u << cn) - 1u;
+        if (can) {
+            u32 m = 0;
+#pragma unroll 1
+            for (u32 j = 0; j < cn; ++j) {   // warp-uniform: broadcast loads
+                const u32 k = c0 + j;
+                if (!culled_point(c.brec[k], c.bmag[k], br, c.bkind[k] == 0u ? kp : kh)) m |= 1u << j;
+            }
+            mask = m;
+            while (m) {   // per lane: the ray-aware bound on the survivors
+                const u32 j = __ffs(m) - 1;
+                m &= m - 1;
+                const u32 k = c0 + j;
+                if (culled<true>(c.brec[k], c.bmag[k], c.bkind[k], br, cull)) mask &= ~(1u << j);
+            }
+        }
+        while (mask) {   // this lane's candidates, in index order
+            const u32 i = c0 + (__ffs(mask) - 1);
+            mask &= mask - 1;
+            if (can && culled_point(c.brec[i], c.bmag[i], br, c.bkind[i] == 0u ? kp : kh)) continue;
+            ++tested;
+            Light<G> cur = l;
+            typename O::Cache cc;
+            hash_usize(c, i);
+            const float dist = O::template detect<W, false>(self + head + i * stride, c, cc, cur);
+            if (dist > -EPSF && (min_dist <= -EPSF || dist < min_dist)) {
+                min_dist = dist; min_index = i; min_hasher = c.hasher;
+                cull = cull_from_dist(dist);
+                kp = point_cut(0, br.t, cull);
+                kh = point_cut(1, br.t, cull);
+            }
+            c.hasher = orig;
+        }
+    }
+    c.culled += n - tested;
+    if (!(min_dist > -EPSF)) return -1.0f;
+    if (F) {
+        const u32 tests = c.tests;
+        hash_usize(c, min_index);
+        O::template detect<W, true>(self + head + min_index * stride, c, cache.inner, l);
+        c.tests = tests;
+        cache.index = min_index;
+    }
+    c.hasher = min_hasher;
+    return min_dist;
+}
+
 // ============================================================================ scene
 template <class G, class V, class O, class B> struct SceneImpl {   // {phantom, view, background, object}
     template <int W> using R = Rec<W, Zst, V, B, O>;
+    typedef O Object;
+    typedef G Geometry;
     template <int W> __host__ __device__ static constexpr u32 static_size() { return R<W>::off(3) + O::template lay<W>().size; }
     // render/scene.inl:16-44 with H = hops; returns the path's emission.
     template <int W>
@@ -1037,6 +1212,10 @@ template <class G, class V, class O, class B> struct SceneImpl {   // {phantom, 
     }
 };
 
+// The element type of a top-level object vector.
+template <class O> struct VecElem { static constexpr bool is_vec = false; typedef Zst T; };
+template <class G, class O> struct VecElem<ObjectVec<G, O>> { static constexpr bool is_vec = true; typedef O T; };
+
 // ============================================================================ kernel
 // One thread per pixel (render/render.cl:6-27); `passes` samples of the pixel in order, the
 // same float additions as `passes` launches of one pass.
@@ -1051,7 +1230,28 @@ __global__ void __launch_bounds__(128, HTG_MIN_BLOCKS) render_generic(Ptr scene,
                                                      u32 hops, u32 passes, u32 flags, float4 *canvas, u32 *seeds,
                                                      unsigned long long *stats, u32 *err) {
     const u32 idx = blockIdx.x * 128u + threadIdx.x;
-    u32 samples = 0, hops_done = 0, hits = 0, tests = 0;
+    u32 samples = 0, hops_done = 0, hits = 0, tests = 0, culled = 0;
+    typedef typename Scene::Object Obj;
+    typedef typename Scene::Geometry Geo;
+    Ptr bvec = nullptr;
+    const float4 *brec = nullptr;
+    const float *bmag = nullptr;
+    const u32 *bkind = nullptr;
+    if constexpr (VecBounds<Geo, typename VecElem<Obj>::T>::ok && VecElem<Obj>::is_vec) {
+        // the top-level object vector's distance bounds, staged once per block
+        __shared__ float4 s_rec[HTG_BOUND_CAP];
+        __shared__ float s_mag[HTG_BOUND_CAP];
+        __shared__ u32 s_kind[HTG_BOUND_CAP];
+        const Ptr vec = scene + Scene::template R<W>::off(3);
+        const u32 nb = stage_vec_bounds<Geo, typename VecElem<Obj>::T, W>(vec, scene + scene_size, s_rec, s_mag, s_kind);
+        __syncthreads();
+        if (nb != 0xFFFFFFFFu) {
+            bvec = vec;
+            brec = s_rec;
+            bmag = s_mag;
+            bkind = s_kind;
+        }
+    }
     if (idx < width * height) {
         const u32 x = idx % width, y = idx / width;
         const float px = (__uint2float_rn(2u * x + 1u) - __uint2float_rn(width)) / __uint2float_rn(height);
@@ -1065,6 +1265,11 @@ __global__ void __launch_bounds__(128, HTG_MIN_BLOCKS) render_generic(Ptr scene,
         c.tests = 0;
         c.end = scene + scene_size;
         c.err = err;
+        c.bvec = bvec;
+        c.brec = brec;
+        c.bmag = bmag;
+        c.bkind = bkind;
+        c.culled = 0;
         float4 acc = canvas[idx];
         for (u32 k = 0; k < passes; ++k) {
             const Col col = Scene::template sample<W>(scene, c, px, py, size, hops, hops_done, hits);
@@ -1074,18 +1279,15 @@ __global__ void __launch_bounds__(128, HTG_MIN_BLOCKS) render_generic(Ptr scene,
         canvas[idx] = acc;
         seeds[idx] = c.rng;
         tests = c.tests;
+        culled = c.culled;
     }
-    if (stats) {   // samples, hops, object tests, hits, evaluated tests (= object tests: no culling)
-        unsigned long long v[4] = {samples, hops_done, tests, hits};
-        for (int k = 0; k < 4; ++k) {
+    if (stats) {   // samples, hops, object tests the reference makes, hits, tests evaluated
+        unsigned long long v[5] = {samples, hops_done, (unsigned long long)tests + culled, hits, tests};
+        for (int k = 0; k < 5; ++k) {
             for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xFFFFFFFFu, v[k], o);
         }
         if ((threadIdx.x & 31u) == 0) {
-            atomicAdd(stats + 0, v[0]);
-            atomicAdd(stats + 1, v[1]);
-            atomicAdd(stats + 2, v[2]);
-            atomicAdd(stats + 3, v[3]);
-            atomicAdd(stats + 4, v[2]);
+            for (int k = 0; k < 5; ++k) atomicAdd(stats + k, v[k]);
         }
     }
 }

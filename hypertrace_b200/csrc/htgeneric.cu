@@ -48,7 +48,7 @@ typedef SceneImpl<Eu, MappedView<Eu, PointView<Eu>, Homogenous3>,
 // ============================================================================ NVRTC / driver
 namespace {
 
-// Header texts for NVRTC (generated from ht_math.cuh and ht_generic.cuh at build time).
+// Header texts for NVRTC (generated from ht_math.cuh, ht_bound.cuh and ht_generic.cuh at build time).
 #include "generated/nvrtc_headers.inc"
 
 typedef int (*nvrtcCreateProgram_t)(void **, const char *, const char *, int, const char *const *, const char *const *);
@@ -183,9 +183,9 @@ int generic_program_build(const char *type_expr, int address_width, char *log, s
                       std::to_string(W) + ">();\n";
     const std::string kname = "&htg::render_generic<htg::UserScene, " + std::to_string(W) + ">";
     void *prog = nullptr;
-    const char *hdr_src[] = {k_header_ht_math, k_header_ht_generic};
-    const char *hdr_name[] = {"ht_math.cuh", "ht_generic.cuh"};
-    if (n.create(&prog, src.c_str(), "user_scene.cu", 2, hdr_src, hdr_name) != 0) return fail(HTC_ERR_CUDA, "nvrtcCreateProgram failed");
+    const char *hdr_src[] = {k_header_ht_math, k_header_ht_bound, k_header_ht_generic};
+    const char *hdr_name[] = {"ht_math.cuh", "ht_bound.cuh", "ht_generic.cuh"};
+    if (n.create(&prog, src.c_str(), "user_scene.cu", 3, hdr_src, hdr_name) != 0) return fail(HTC_ERR_CUDA, "nvrtcCreateProgram failed");
     n.add_name(prog, kname.c_str());
     const char *opts[] = {"-arch=sm_100a", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
                           "-ftz=false", "-lineinfo", "-default-device"};
