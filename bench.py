@@ -45,21 +45,22 @@ import numpy as np  # noqa: E402
 METRIC = "Msamples/s at 1080p hyperbolic (1920x1080, 200 objects, H=8)"
 UNIT = "Msamples/s"
 
-# Executed FP32 operations per unit of work in the CUDA path (static tally of the source,
-# each add/sub/mul/div/sqrt/log/sin/cos = 1).
-FLOPS_PER_EXACT_TEST = 219      # one inverse ray map (204) + shape distance test lower bound (15)
-FLOPS_PER_BOUND_TEST = 12       # world-space point bound of one object (hops x objects of them)
-FLOPS_PER_HIT_HOP = 936         # winner recompute + map back + interact maps + material
-FLOPS_PER_SAMPLE = 120          # camera ray
-FLOPS_PER_ESTIMATE = 30         # upper estimate of the nearest crossing, per object of the first chunk and hop
-ESTIMATE_OBJECTS = 32           # objects the estimate looks at (the first chunk)
-# The reference's own count (two ray maps of 256 ops per candidate: object/mapped.inl:32,34).
-REF_FLOPS_PER_OBJECT_TEST = 527
-# DRAM bytes per path advanced by one render_wave launch: dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of the hop-depth-1 launch of this frame (156.3 MB +
-# 93.1 MB for 2,073,600 paths; profiles/render_wave_hy1080p_200obj.md): the 68-byte ray state
-# read, the survivors' 68 bytes written, canvas and seed of the paths that end.
-DRAM_BYTES_PER_HOP = (156.262144e6 + 93.144064e6) / 2073600
+# Measured per path advanced by render_wave on this frame: one ncu capture of the 8 launches
+# of one pass (hop depths 0-7) of `python bench.py --steps 1 --warmup 1 --no-extras --no-e2e
+# --no-cpu-baseline`, each counter summed over the 8 launches and divided by the pass's path-hops
+# (1920 x 1080 x hops per sample of that run). FP32 operations count 2 per FFMA, 1 per FADD /
+# FMUL, twice that for their packed forms (FFMA2 / FADD2 / FMUL2); instructions are warp
+# instructions issued; DRAM bytes are read + written. Frozen from that capture (the summary with
+# the command is profiles/render_wave_hy1080p_200obj.md): re-capture after a kernel change.
+FP32_OPS_PER_HOP = None
+WARP_INSTR_PER_HOP = None
+DRAM_BYTES_PER_HOP = None
+# The reference's own FP32 count per hop for comparison: every object's detect maps the ray in
+# and out (two ray maps of 256 operations, object/mapped.inl:32,34, plus the shape test), i.e.
+# 527 per object and hop. Distance culling skips 98 % of those tests, so this count can exceed
+# the chip's peak: it measures how much of the reference's algorithm each second covers, not
+# how busy the FP32 pipes are.
+REF_OPS_PER_OBJECT_TEST = 527
 
 
 def parse_args():
@@ -358,13 +359,12 @@ def main():
     all_samples, max_s, all_hops = replicas.aggregate(samples, dev_s, hops, device=dev)
     value = all_samples / max_s / 1e6
 
-    # roofline of render_wave (one launch per hop depth, `passes * hops` launches per step)
+    # roofline of render_wave (one launch per hop depth, `passes * hops` launches per step):
+    # measured operations per path-hop x this run's path-hops, over the device time
     launches = args.steps * args.passes * sc.hops
-    exec_flops = (exact * FLOPS_PER_EXACT_TEST + tests * FLOPS_PER_BOUND_TEST + hits * FLOPS_PER_HIT_HOP
-                  + samples * FLOPS_PER_SAMPLE + hops * min(ESTIMATE_OBJECTS, sc.n_objects) * FLOPS_PER_ESTIMATE)
-    ref_flops = tests * REF_FLOPS_PER_OBJECT_TEST + hits * FLOPS_PER_HIT_HOP + samples * FLOPS_PER_SAMPLE
     per_launch_s = dev_s / launches
-    achieved = exec_flops / launches / per_launch_s / 1e12
+    achieved = FP32_OPS_PER_HOP * hops / dev_s / 1e12 if FP32_OPS_PER_HOP else None
+    ref_tflops = tests * REF_OPS_PER_OBJECT_TEST / dev_s / 1e12
 
     # ---------------- the persistent kernel (all passes in one launch) on the same frame,
     # through the entry point that still uses it, for comparison
@@ -466,13 +466,21 @@ def main():
             "hops_per_sample": hops / max(samples, 1),
             "exact_tests_per_hop": exact / max(hops, 1),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak_tflops if fp32_peak_tflops else None,
-                         "traffic": DRAM_BYTES_PER_HOP * hops / launches,
-                         "traffic_source": "bytes per launch: the ncu capture's DRAM bytes per path of the "
-                                           "hop-1 launch x this run's paths per launch (hops / launches)",
+                         "frac": achieved / fp32_peak_tflops if achieved and fp32_peak_tflops else None,
+                         "traffic": DRAM_BYTES_PER_HOP * hops / launches if DRAM_BYTES_PER_HOP else None,
+                         "source": "FP32 operations and DRAM bytes per path-hop: constants from one ncu "
+                                   "capture of a pass's 8 launches (ffma x2 + fadd + fmul, packed forms x2), "
+                                   "times this run's path-hops; traffic per launch",
                          "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",
-                         "flops_per_launch": exec_flops / launches,
-                         "reference_count_tflops": ref_flops / launches / per_launch_s / 1e12},
+                         "issue": {"achieved_ginstr_per_s": WARP_INSTR_PER_HOP * hops / dev_s / 1e9
+                                   if WARP_INSTR_PER_HOP else None,
+                                   "peak_ginstr_per_s": 148 * 4 * (clk.get("sm_mhz") or 1965.0) / 1e3,
+                                   "note": "warp instructions issued (the kernel is issue-bound) against one per "
+                                           "cycle per SM sub-partition at the sampled SM clock"},
+                         "reference_count_tflops": ref_tflops,
+                         "reference_count_note": "the reference's FP32 count (527 per object test, hops x "
+                                                 "objects tests) over the same time: above the peak because "
+                                                 "culling skips 98 % of those tests"},
             "parity": parity,
             "batched": batched,
             "serving": serving,
