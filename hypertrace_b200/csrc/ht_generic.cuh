@@ -1060,10 +1060,14 @@ template <class... O> struct BoundKind<ObjectChoice<Hy, O...>> {
 
 // A vector of Moebius-mapped objects of a known shape gets distance bounds: one world-space
 // record per element (stage_bound of the element's map) in shared memory, staged once per
-// block by render_generic when the vector is the scene's top-level object and holds at most
-// HTG_BOUND_CAP elements.
+// block by render_generic when the vector is the scene's top-level object and holds between
+// HTG_BOUND_MIN and HTG_BOUND_CAP elements (below 32 the bound arithmetic costs more than the
+// exact tests it saves: the hy.rs example's 4 objects ran 625 Msamples/s with it, 644 without).
 #ifndef HTG_BOUND_CAP
 #define HTG_BOUND_CAP 256u
+#endif
+#ifndef HTG_BOUND_MIN
+#define HTG_BOUND_MIN 32u
 #endif
 template <class G, class O> struct VecBounds { static constexpr bool ok = false; };
 template <class X> struct VecBounds<Hy, MappedObject<Hy, X, Moebius>> {
@@ -1074,14 +1078,17 @@ template <class X> struct VecBounds<Hy, MappedObject<Hy, X, Moebius>> {
     template <int W> HT_D static Mo map_of(Ptr elem) { return Moebius::load(elem + Rec<W, Zst, Moebius, X>::off(1)); }
 };
 // Stages the records of the vector at `self` (all threads of the block; returns the element
-// count staged, or 0xFFFFFFFF when the vector is too large or its count does not fit the bytes).
+// count staged, or 0xFFFFFFFF when the vector is too small or too large for the bounds or its
+// count does not fit the bytes).
 template <class G, class O, int W>
 HT_D u32 stage_vec_bounds(Ptr self, Ptr end, float4 *rec, float *mag, u32 *kind) {
     typedef VecBounds<G, O> B;
     constexpr u32 stride = O::template lay<W>().size;
     constexpr u32 head = upm((u32)W, O::template lay<W>().align);
     const u32 n = ldusize<W>(self);
-    if (stride == 0 || end < self + head || n > (u32)((end - self - head) / stride) || n > HTG_BOUND_CAP) return 0xFFFFFFFFu;
+    if (stride == 0 || end < self + head || n > (u32)((end - self - head) / stride) || n > HTG_BOUND_CAP ||
+        n < HTG_BOUND_MIN)
+        return 0xFFFFFFFFu;
     const float nan = __int_as_float(0x7fc00000);
     for (u32 i = threadIdx.x; i < n; i += blockDim.x) {
         const Ptr elem = self + head + i * stride;

@@ -4,8 +4,8 @@
 // library (kernel/ocl/algebra/*.cc, transform/*.cc) so that, compiled with FMA
 // contraction off (-fmad=false) and IEEE division / square root, each result is
 // bit-identical to the reference compiled for the host. Transcendentals are the
-// exception: log, cos and sin are evaluated in FP64 and rounded once (see below), which is
-// what the host libm's float versions return in all but a small fraction of cases.
+// exception: logf is CUDA's, cos and sin are evaluated in FP64 and rounded once (see below);
+// the host libm's float versions return other values on a small fraction of arguments.
 #pragma once
 #ifdef __CUDACC_RTC__
 // Runtime compilation (NVRTC) has no C++ standard headers; these are the only ones used.
@@ -226,12 +226,12 @@ HT_D float hy_x(Q4 a, Q4 b) {
     Q4 d = q_sub(a, b);
     return 1.0f + dot4(d, d) / (2.0f * a.z * b.z);
 }
-// The logarithm is evaluated in FP64 and rounded once, like cos/sin below: the host libm's
-// logf lands on that value (0 differences in the C restatement over the 1080p frame's paths),
-// CUDA's single-precision logf does not always, and each difference can flip a nearest-hit
-// tie and with it the rest of the path.
+// CUDA's single-precision logf. Evaluating it in FP64 and rounding once (what the host libm's
+// logf returns) was measured: the share of pixels that differ from the reference over 16
+// passes of the 1080p frame stayed 0.365 % (the flips come from cos / sin, below), and the
+// headline kernel lost 4.5 % (the generic kernel 30 %).
 HT_D float hy_dist_from_x(float x) {
-    return (float)log((double)(x + sqrtf(x * x - 1.0f)));
+    return logf(x + sqrtf(x * x - 1.0f));
 }
 HT_D float hy_distance(Q4 a, Q4 b) { return hy_dist_from_x(hy_x(a, b)); }
 HT_D Q4 hy_dir_at(Q4 p, Q4 d, Q4 h) {

@@ -20,6 +20,7 @@ one-pass kernel (the shape of the reference's Pipeline loop).
 """
 from __future__ import annotations
 
+import collections
 import ctypes
 import dataclasses
 import time
@@ -110,6 +111,8 @@ class Server:
         self.gamma = gamma
         self.steps = 0
         self.device_s = 0.0
+        self.feed = 32              # requests handed to the native server ahead of admission
+        self._pinned = {}           # pinned host buffers by (size, dtype), reused across requests
         h = ctypes.c_void_p()
         _lib.call("htc_server_create", hbm_budget_bytes, step_samples, max_views, ctypes.byref(h))
         self.handle = h
@@ -127,15 +130,23 @@ class Server:
                 pass
             self.handle = None
 
+    def _buffer(self, n: int, dtype) -> torch.Tensor:
+        free = self._pinned.get((n, dtype))
+        return free.pop() if free else torch.empty(n, dtype=dtype, pin_memory=True)
+
+    def _release(self, out: Dict[str, torch.Tensor]) -> None:
+        for t in out.values():
+            self._pinned.setdefault((t.numel(), t.dtype), []).append(t)
+
     def _submit(self, r: Request, keep_images: bool) -> int:
         v = r.view
         data = v.scene.to_bytes()
         w, h = v.width, v.height
         r._scene = np.frombuffer(data, dtype=np.uint8).copy()   # type: ignore[attr-defined]
-        r._out = {"image": torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)}   # type: ignore[attr-defined]
+        r._out = {"image": self._buffer(w * h * 4, torch.uint8)}   # type: ignore[attr-defined]
         if keep_images:
-            r._out["canvas"] = torch.empty(w * h * 4, dtype=torch.float32, pin_memory=True)
-            r._out["seeds"] = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
+            r._out["canvas"] = self._buffer(w * h * 4, torch.float32)
+            r._out["seeds"] = self._buffer(w * h, torch.int32)
         req = _lib.HtcRequest(r._scene.ctypes.data, len(data), w, h, v.scene.recipe, v.scene.hops, v.flags, 32,
                               v.spp, v.global_seed & 0xFFFFFFFF,
                               _lib.HTC_PRIORITY_INTERACTIVE if r.kind == INTERACTIVE else _lib.HTC_PRIORITY_BATCH,
@@ -151,9 +162,13 @@ class Server:
         return rid.value
 
     def run(self, requests: Sequence[Request], keep_images: bool = False) -> Dict[str, object]:
-        """Serve `requests` in real time (arrival times relative to the call)."""
+        """Serve `requests` in real time (arrival times relative to the call). Arrivals wait
+        in two host queues (interactive first) and are handed to the native server while it
+        holds fewer than `feed` requests not yet admitted, so that a burst of arrivals costs
+        one loop turn a few submissions at a time."""
         arrivals = sorted(requests, key=lambda r: r.arrival)
         ai, done = 0, 0
+        pending = {INTERACTIVE: collections.deque(), BATCH: collections.deque()}
         by_id: Dict[int, Request] = {}
         ids = (ctypes.c_uint64 * 256)()
         n = ctypes.c_uint32()
@@ -165,13 +180,19 @@ class Server:
         while done < len(arrivals):
             now = time.perf_counter() - t0
             while ai < len(arrivals) and arrivals[ai].arrival <= now:
-                r = arrivals[ai]
+                pending[arrivals[ai].kind].append(arrivals[ai])
                 ai += 1
-                rid = self._submit(r, keep_images)
-                if rid:
-                    by_id[rid] = r
-                else:
-                    done += 1
+            _lib.call("htc_server_stats", self.handle, ctypes.byref(info))
+            room = self.feed - info.waiting
+            for q in (pending[INTERACTIVE], pending[BATCH]):
+                while q and room > 0:
+                    r = q.popleft()
+                    rid = self._submit(r, keep_images)
+                    if rid:
+                        by_id[rid] = r
+                        room -= 1
+                    else:
+                        done += 1
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             _lib.call("htc_server_step", self.handle, self.ctx.stream(), ctypes.byref(rendered))
@@ -191,10 +212,12 @@ class Server:
                     r.image = r._out["image"].numpy().reshape(h, w, 4).copy()
                     r.canvas = r._out["canvas"].numpy().reshape(h, w, 4).copy()   # type: ignore[attr-defined]
                     r.seeds = r._out["seeds"].numpy().view(np.uint32).reshape(h, w).copy()   # type: ignore[attr-defined]
+                self._release(r._out)   # type: ignore[attr-defined]
                 r._out = None   # type: ignore[attr-defined]
             if not rendered.value:
                 _lib.call("htc_server_stats", self.handle, ctypes.byref(info))
-                if info.in_flight == 0 and info.active == 0 and info.waiting == 0 and ai < len(arrivals):
+                idle = not pending[INTERACTIVE] and not pending[BATCH]
+                if idle and info.in_flight == 0 and info.active == 0 and info.waiting == 0 and ai < len(arrivals):
                     time.sleep(max(0.0, min(arrivals[ai].arrival - (time.perf_counter() - t0), 0.005)))
                 elif info.in_flight:
                     time.sleep(0.0002)
