@@ -52,9 +52,9 @@ UNIT = "Msamples/s"
 # FMUL, twice that for their packed forms (FFMA2 / FADD2 / FMUL2); instructions are warp
 # instructions issued; DRAM bytes are read + written. Frozen from that capture (the summary with
 # the command is profiles/render_wave_hy1080p_200obj.md): re-capture after a kernel change.
-FP32_OPS_PER_HOP = None
-WARP_INSTR_PER_HOP = None
-DRAM_BYTES_PER_HOP = None
+FP32_OPS_PER_HOP = 6288.7       # 61.70e9 per pass over 9.81e6 path-hops
+WARP_INSTR_PER_HOP = 493.42     # 4.841e9 per pass
+DRAM_BYTES_PER_HOP = 114.92     # 1.127e9 per pass
 # The reference's own FP32 count per hop for comparison: every object's detect maps the ray in
 # and out (two ray maps of 256 operations, object/mapped.inl:32,34, plus the shape test), i.e.
 # 527 per object and hop. Distance culling skips 98 % of those tests, so this count can exceed
@@ -475,6 +475,8 @@ def main():
                          "issue": {"achieved_ginstr_per_s": WARP_INSTR_PER_HOP * hops / dev_s / 1e9
                                    if WARP_INSTR_PER_HOP else None,
                                    "peak_ginstr_per_s": 148 * 4 * (clk.get("sm_mhz") or 1965.0) / 1e3,
+                                   "frac": WARP_INSTR_PER_HOP * hops / dev_s / 1e9
+                                   / (148 * 4 * (clk.get("sm_mhz") or 1965.0) / 1e3) if WARP_INSTR_PER_HOP else None,
                                    "note": "warp instructions issued (the kernel is issue-bound) against one per "
                                            "cycle per SM sub-partition at the sampled SM clock"},
                          "reference_count_tflops": ref_tflops,
