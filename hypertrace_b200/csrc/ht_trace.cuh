@@ -131,7 +131,6 @@ struct StagedScene {
     const float *mag;        // shared, 1 per slot: BOUND_EPS * max |bound component|
     const uint32_t *orig;    // shared, 1 per slot: the object's index in the scene
     float4 *win;             // shared, this thread's 2 float4: the scan winner's local ray
-    float4 *task;            // shared, 2 float4 per thread of the block: pooled exact tests' local rays
     const uint8_t *objects;  // global, OBJ_STRIDE per object (forward maps, materials), by scene index
     uint32_t n;              // objects
     uint32_t ns;             // slots: n, plus the dummy slot of a hyperbolic scene with an odd plane count
@@ -265,11 +264,9 @@ HT_D float upper_estimate(const StagedScene &s, const BoundRay &r, uint32_t prev
     return best < __int_as_float(0x7f800000) ? dist_from_e2(best) : best;
 }
 
-// POOL: the exact tests of a chunk are pooled across the warp (every lane of the warp calls
-// together; `alive` = false for lanes without a path, which then have no candidates).
-template <bool OOL, bool POOL = false>
+template <bool OOL>
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
-                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact, bool alive = true) {
+                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact) {
     // Nearest hit with ties to the lowest scene index (object/vector.inl:37-50): candidates
     // are compared on (distance, index), so the order of the slots does not matter; x =
     // cosh(distance) is compared first and the logarithm taken only when x can win; objects
@@ -278,11 +275,9 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
     float min_x = __int_as_float(0x7f800000);   // +inf
     uint32_t kmin = 0, kmin_orig = 0xFFFFFFFFu;
     const Q4 p = ray.p, v = ray.v;
-    const bool can_cull = alive && cull_point_ok(p);
+    const bool can_cull = cull_point_ok(p);
     const BoundRay br = bound_ray(p, v);
     const PairRay pr = pair_ray(br);
-    const uint32_t lane = threadIdx.x & 31u;
-    float4 *const task_warp = s.task + 2u * (threadIdx.x & ~31u);   // this warp's task scratch
     Cull cull = cull_none();
     if (can_cull) {   // a threshold before the first exact test, from the first slots' crossings
         const float u = upper_estimate(s, br, prev_hash);
@@ -293,7 +288,7 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
         const uint32_t cn = min(32u, s.ns - c0);
         uint32_t valid = cn == 32 ? 0xFFFFFFFFu : (1u << cn) - 1u;
         if (s.dummy - c0 < 32u) valid &= ~(1u << (s.dummy - c0));
-        uint32_t mask = alive ? valid : 0u;
+        uint32_t mask = valid;
         if (can_cull) {
             mask = 0;
             // kept rolled: the kernel is bound by instruction fetch as much as by issue
@@ -312,93 +307,6 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
                 const uint32_t q = c0 + j;
                 if (culled<OOL>(s.bound[q], s.mag[q], s.shape[q], br, cull)) mask &= ~(1u << j);
             }
-        }
-        if constexpr (POOL) {
-            // Rounds of up to 32 (owner, candidate) pairs: the warp's candidates in lane order,
-            // task t to lane t. Each owner compares the results of its tasks on (distance,
-            // scene index) and, when its threshold tightened, drops the candidates the cheap
-            // bound now culls before the next round.
-            bool dirty = false;
-            for (;;) {
-                if (dirty && can_cull) {
-                    uint32_t m = mask;
-                    while (m) {
-                        const uint32_t j = __ffs(m) - 1;
-                        m &= m - 1;
-                        if (culled_slot(s, c0 + j, br, kp, kh)) mask &= ~(1u << j);
-                    }
-                }
-                dirty = false;
-                const uint32_t cnt = __popc(mask);
-                uint32_t incl = cnt;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= (uint32_t)o) incl += y;
-                }
-                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-                if (total == 0) break;
-                const uint32_t excl = incl - cnt;
-                // owner of task `lane`: the first lane whose inclusive count exceeds it
-                uint32_t lo = 0, hi = 31;
-#pragma unroll
-                for (int step = 0; step < 5; ++step) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (__shfl_sync(0xffffffffu, incl, mid) > lane) hi = mid;
-                    else lo = mid + 1;
-                }
-                const uint32_t owner = lo;
-                const uint32_t o_excl = __shfl_sync(0xffffffffu, excl, owner);
-                const uint32_t o_mask = __shfl_sync(0xffffffffu, mask, owner);
-                const uint32_t o_prev = __shfl_sync(0xffffffffu, prev_hash, owner);
-                Q4 op, ov;
-                op.x = __shfl_sync(0xffffffffu, p.x, owner); op.y = __shfl_sync(0xffffffffu, p.y, owner);
-                op.z = __shfl_sync(0xffffffffu, p.z, owner); op.w = __shfl_sync(0xffffffffu, p.w, owner);
-                ov.x = __shfl_sync(0xffffffffu, v.x, owner); ov.y = __shfl_sync(0xffffffffu, v.y, owner);
-                ov.z = __shfl_sync(0xffffffffu, v.z, owner); ov.w = __shfl_sync(0xffffffffu, v.w, owner);
-                float tdist = -1.0f;
-                uint32_t tq = 0, tk = 0xFFFFFFFFu;
-                if (lane < total) {
-                    tq = c0 + (__fns(o_mask, 0, (int)(lane - o_excl) + 1));
-                    tk = s.orig[tq];
-                    const uint32_t shape = s.shape[tq];
-                    const bool repeat = (tk == o_prev);
-                    if (!(shape == 0 && repeat)) {   // a geodesic plane is never hit twice in a row
-                        ++n_exact;
-                        HyRay l = ray_hy_map_call(mo_from(s.inv[2 * tq], s.inv[2 * tq + 1]), op, ov);
-                        const float x = shape == 0 ? plane_hy_x(l.p, l.v) : horosphere_x(l.p, l.v, repeat);
-                        if (x >= 1.0f) {
-                            tdist = hy_dist_from_x(x);
-                            task_warp[2 * lane] = make_float4(l.p.x, l.p.y, l.p.z, l.p.w);
-                            task_warp[2 * lane + 1] = make_float4(l.v.x, l.v.y, l.v.z, l.v.w);
-                        }
-                    }
-                }
-                __syncwarp();
-                // each owner takes the results of its tasks of this round, in task order
-                const uint32_t mine = incl > 32u ? (excl < 32u ? 32u - excl : 0u) : cnt;
-                const uint32_t rounds = __reduce_max_sync(0xffffffffu, mine);
-                for (uint32_t r = 0; r < rounds; ++r) {
-                    const uint32_t src = min(excl + r, 31u);
-                    const float d = __shfl_sync(0xffffffffu, tdist, src);
-                    const uint32_t kk = __shfl_sync(0xffffffffu, tk, src);
-                    const uint32_t qq = __shfl_sync(0xffffffffu, tq, src);
-                    if (r < mine && d > -EPSF && (min_dist <= -EPSF || d < min_dist || (d == min_dist && kk < kmin_orig))) {
-                        min_dist = d;
-                        kmin = qq;
-                        kmin_orig = kk;
-                        cull = cull_from_dist(d);
-                        kp = point_cut(0, br.t, cull);
-                        kh = point_cut(1, br.t, cull);
-                        dirty = true;
-                        s.win[0] = task_warp[2 * src];
-                        s.win[1] = task_warp[2 * src + 1];
-                    }
-                }
-                for (uint32_t r = 0; r < mine; ++r) mask &= mask - 1;   // this round's candidates are done
-                __syncwarp();
-            }
-            continue;
         }
         while (mask) {   // this lane's candidates, in slot order
             const uint32_t q = c0 + (__ffs(mask) - 1);

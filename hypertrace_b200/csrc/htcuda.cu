@@ -48,11 +48,6 @@ thread_local std::string g_last_error;
 #ifndef HT_PLAIN_MINB
 #define HT_PLAIN_MINB 7
 #endif
-// Wavefront kernels of hyperbolic scenes: 1 = pool each chunk's exact object tests across the
-// warp, 0 = each lane tests its own candidates.
-#ifndef HT_POOL
-#define HT_POOL 0
-#endif
 // htc_render_passes: 2 = wavefronts (one launch per hop depth), 1 = the persistent kernel,
 // 0 = one launch of the one-pass kernel per pass. All three give the same bits. Measured at
 // 1920x1080 / 200 objects / H = 8 (Msamples/s): wavefronts 286.9, one-pass kernel 239.3,
@@ -111,7 +106,6 @@ struct SceneSmem {
     uint32_t *shape, *orig;
     float *mag;
     float4 *win;
-    float4 *task;
     float4 *end;   // first float4 past the layout
 };
 __host__ __device__ constexpr uint32_t scene_slots(uint32_t n) { return n + 1; }
@@ -130,8 +124,7 @@ __device__ __forceinline__ SceneSmem carve_scene(float4 *smem, uint32_t n) {
     c.mag = reinterpret_cast<float *>(c.shape + ns);
     c.orig = reinterpret_cast<uint32_t *>(c.mag + ns);
     c.win = smem + scene_win_offset(n) / 16;
-    c.task = c.win + 2 * BLOCK_THREADS;
-    c.end = c.task + 2 * BLOCK_THREADS;
+    c.end = c.win + 2 * BLOCK_THREADS;
     return c;
 }
 
@@ -264,7 +257,6 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
     s.mag = sm.mag;
     s.orig = sm.orig;
     s.win = sm.win + 2 * tid;
-    s.task = sm.task;
     s.objects = objects;
     s.n = n;
     s.ns = n + (dummy != 0xFFFFFFFFu ? 1u : 0u);
@@ -288,11 +280,11 @@ __device__ __forceinline__ typename PathOf<R>::T camera(const StagedScene &s, fl
     if constexpr (R == RECIPE_HY) return camera_hy(s, px, py, size, rng, flags);
     else return camera_eu(s, px, py, size, rng, flags);
 }
-template <int R, bool OOL = true, bool POOL = false>
+template <int R, bool OOL = true>
 __device__ __forceinline__ bool hop(const StagedScene &s, typename PathOf<R>::T &ray, uint32_t &rng,
                                     uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit,
-                                    uint32_t &n_exact, bool alive = true) {
-    if constexpr (R == RECIPE_HY) return hop_hy<OOL, POOL>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact, alive);
+                                    uint32_t &n_exact) {
+    if constexpr (R == RECIPE_HY) return hop_hy<OOL>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
     else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
 }
 
@@ -571,45 +563,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
     Col intensity = {1.0f, 1.0f, 1.0f};
     Col emission = {0.0f, 0.0f, 0.0f};
     const bool first = FH == 1 || (FH == 0 && first_hop);
-    constexpr bool pool = HT_POOL && R == RECIPE_HY;
-    if constexpr (pool) {   // every lane calls the hop (pooled exact tests); lanes past the queue are dead
-        const bool alive = i < n;
-        if (alive) {
-            if (first) {
-                pixel = i;
-                float px, py, size;
-                pixel_pos(i % W, i / W, W, H, px, py, size);
-                rng = seeds[i];
-                ray = camera<R>(s, px, py, size, rng, flags);
-            } else {
-                ray = path_load<R>(in.p[i], in.v[i]);
-                const float4 t = in.t[i], e = in.e[i];
-                intensity.x = t.x; intensity.y = t.y; intensity.z = t.z;
-                rng = __float_as_uint(t.w);
-                emission.x = e.x; emission.y = e.y; emission.z = e.z;
-                pixel = __float_as_uint(e.w);
-                prev_hash = in.h[i];
-            }
-        } else {
-            ray = path_load<R>(make_float4(0.0f, 0.0f, 1.0f, 0.0f), make_float4(0.0f, 0.0f, 1.0f, 0.0f));
-        }
-        __syncwarp();
-        bool hit;
-        const bool go = hop<R, OOL, true>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact, alive);
-        if (alive) {
-            st.hops += 1;
-            st.tests += s.n;
-            st.hits += hit ? 1 : 0;
-            cont = go && !last_hop;
-            if (!cont) {
-                st.samples += 1;
-                float4 c = canvas[pixel];
-                c.x += emission.x; c.y += emission.y; c.z += emission.z; c.w += 1.0f;
-                canvas[pixel] = c;
-                seeds[pixel] = rng;
-            }
-        }
-    } else if (i < n) {
+    if (i < n) {
         if (first) {
             pixel = i;
             float px, py, size;
@@ -985,7 +939,7 @@ static int check_program(const htc_program *p) {
     return HTC_OK;
 }
 static size_t smem_bytes(uint32_t max_objects) {   // carve_scene's layout
-    return scene_win_offset(max_objects) + 4u * 16u * BLOCK_THREADS;
+    return scene_win_offset(max_objects) + 2u * 16u * BLOCK_THREADS;
 }
 static uint32_t objects_capacity(int recipe, size_t scene_size) {
     const size_t hdr = recipe == HTC_RECIPE_HY ? Layout<RECIPE_HY>::OBJECTS : Layout<RECIPE_EU>::OBJECTS;
