@@ -80,7 +80,13 @@ int htc_set_device(int device);
 
 /* Replaces Render::new (processing/src/render.rs:72-100): selects the compiled kernel
  * family for a scene recipe and light-hop count H (objects/src/scene.rs:21,64).
- * address_width: 32 or 64 (types/src/config.rs:18-31); double_support must be 0. */
+ * address_width: 32 or 64 (types/src/config.rs:18-31). double_support (types/src/config.rs:
+ * 38-43) != 0 is served for HTC_RECIPE_HY and HTC_RECIPE_EU: the scene bytes are in the
+ * double_support layout (8-byte f64 fields, f64 vectors and maps aligned to their size), and
+ * every render call narrows them on the device to the f32 layout (each f64 rounded to the
+ * nearest f32, the value the reference serializes without double_support) into a buffer the
+ * program keeps, then transports in FP32 -- the result is bit for bit that of the f32
+ * serialization; an object count the buffer cannot hold is reported by htc_program_check. */
 int htc_program_create(int recipe, uint32_t light_hops, int address_width, int double_support,
                        uint32_t flags, htc_program **out);
 void htc_program_destroy(htc_program *program);
