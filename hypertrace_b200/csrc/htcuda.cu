@@ -38,15 +38,16 @@ using namespace ht;
 thread_local std::string g_last_error;
 
 // Minimum resident blocks per SM requested from ptxas for the render kernels (register cap).
-// The scan is latency-bound on dependent FP32 chains, so resident warps matter more than the
-// few spilled values of the cold per-path state. Measured at 1080p / 200 objects: the plain
-// kernel 7 blocks (72 registers) 239.5 Msamples/s against 6: 232, 8: 231, 5: 229; the
-// persistent and batched kernels 6.
+// The scan is latency-bound on dependent FP32 chains, so resident warps matter, but the
+// packed point-bound loop and the slot bookkeeping hold more values than the earlier scan.
+// Measured on the current code at 1080p / 200 objects (Msamples/s, 7 -> 6 blocks, i.e. 72 ->
+// 80 registers): wavefront 368.6 -> 373.6, one-pass 288.6 -> 296.9, the batched mix (spp / 16)
+// 994 -> 1014; the earlier scan had measured 7 best (239.5 against 232 for 6).
 #ifndef HT_PERSIST_MINB
 #define HT_PERSIST_MINB 6
 #endif
 #ifndef HT_PLAIN_MINB
-#define HT_PLAIN_MINB 7
+#define HT_PLAIN_MINB 6
 #endif
 // htc_render_passes: 2 = wavefronts (one launch per hop depth), 1 = the persistent kernel,
 // 0 = one launch of the one-pass kernel per pass. All three give the same bits. Measured at
