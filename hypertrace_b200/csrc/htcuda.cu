@@ -40,14 +40,18 @@ thread_local std::string g_last_error;
 // Minimum resident blocks per SM requested from ptxas for the render kernels (register cap).
 // The scan is latency-bound on dependent FP32 chains, so resident warps matter, but the
 // packed point-bound loop and the slot bookkeeping hold more values than the earlier scan.
-// Measured on the current code at 1080p / 200 objects (Msamples/s, 7 -> 6 blocks, i.e. 72 ->
-// 80 registers): wavefront 368.6 -> 373.6, one-pass 288.6 -> 296.9, the batched mix (spp / 16)
-// 994 -> 1014; the earlier scan had measured 7 best (239.5 against 232 for 6).
+// Measured on the current code at 1080p / 200 objects (Msamples/s): 7 -> 6 -> 5 blocks (72 ->
+// 80 -> 96 registers) took the wavefront kernel 368.6 -> 373.2 -> 377.4 and the batched mix
+// (spp / 16) 994 -> 1012 -> 1019; the one-pass kernel 288.6 -> 296.5 -> 295.6. The earlier
+// scan had measured 7 best (239.5 against 232 for 6).
 #ifndef HT_PERSIST_MINB
 #define HT_PERSIST_MINB 6
 #endif
 #ifndef HT_PLAIN_MINB
 #define HT_PLAIN_MINB 6
+#endif
+#ifndef HT_WAVE_MINB
+#define HT_WAVE_MINB 5
 #endif
 // htc_render_passes: 2 = wavefronts (one launch per hop depth), 1 = the persistent kernel,
 // 0 = one launch of the one-pass kernel per pass. All three give the same bits. Measured at
@@ -613,7 +617,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
 // ctr[0]: slots taken by warps of this launch; ctr[1]: paths appended to `out`.
 // in_count: paths in `in` (NULL for hop 0, which covers the W*H pixels).
 template <int R, int FH>
-__global__ void __launch_bounds__(128, HT_PLAIN_MINB) render_wave(
+__global__ void __launch_bounds__(128, HT_WAVE_MINB) render_wave(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
     uint32_t W, uint32_t H, uint32_t hops, uint32_t hop_index, uint32_t flags, float4 *__restrict__ canvas,
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err, WaveQueue in, const uint32_t *in_count,
@@ -673,7 +677,7 @@ __device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_
 // RF = 0 serves views of either recipe (a runtime branch per tile); RF = RECIPE_HY or
 // RECIPE_EU compiles one recipe only (its views alone in `order`), with fewer registers.
 template <int RF, int FH>
-__global__ void __launch_bounds__(128, RF ? HT_PLAIN_MINB : HT_PERSIST_MINB) render_batch_wave(
+__global__ void __launch_bounds__(128, RF ? HT_WAVE_MINB : HT_PERSIST_MINB) render_batch_wave(
     const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
     uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
     uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err) {

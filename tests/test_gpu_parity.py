@@ -233,8 +233,9 @@ def test_pack_bytes_equal_oracle(built):
     assert bad.size == 0, f"{bad.size} pixels differ, first {img[bad[:4]]} -> {got[bad[:4]]} vs {want[bad[:4]]}"
 
 
+@pytest.mark.parametrize("aw", [32, 64])
 @pytest.mark.parametrize("cfg", ["config1", "config0"])
-def test_double_support_scene_renders_as_its_f32_serialization(built, cfg):
+def test_double_support_scene_renders_as_its_f32_serialization(built, cfg, aw):
     """A scene serialized with double_support (8-byte f64 fields, f64 vectors and maps aligned
     to their size) is narrowed on the device to the f32 layout, each f64 rounded to the
     nearest f32 -- what the reference serializes without double_support -- and renders bit
@@ -243,7 +244,7 @@ def test_double_support_scene_renders_as_its_f32_serialization(built, cfg):
     W, H = 96, 64
     out = []
     for double in (False, True):
-        ctx = P.Context(0, P.Config(double_support=double))
+        ctx = P.Context(0, P.Config(address_width=aw, double_support=double))
         buf = P.EntityBuffer(ctx, wl.scene)
         r = P.Render(ctx, wl.scene.recipe, wl.scene.hops)
         a = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
