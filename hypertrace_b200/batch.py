@@ -137,10 +137,12 @@ def config3(seed: int = 0x5EED0003, n_views: int = 96, spp_scale: float = 1.0) -
 
 def autotune(renderer: BatchRenderer, views: Sequence[View], passes: int = 1,
              tiles: Sequence[int] = (256, 512, 1024, 2048),
-             residency: Sequence[int] = (5, 6, 7)) -> Tuple[int, int, dict]:
+             residency: Sequence[int] = (3, 4, 5)) -> Tuple[int, int, dict]:
     """Times one launch of `passes` passes per candidate (tile size x blocks per SM) on the
     views themselves and returns the fastest (tile_pixels, blocks_per_sm, timings). The
-    canvases and seeds are restored afterwards, so tuning leaves no trace in the results."""
+    canvases and seeds are restored afterwards, so tuning leaves no trace in the results.
+    Blocks per SM above the kernels' occupancy limit (5 resident blocks of 128 threads at
+    their register cap) launch as that limit, so the default candidates stop there."""
     saved = [(v.canvas.image.clone(), v.canvas.seeds.clone()) for v in views]
     timings = {}
     stream = torch.cuda.current_stream(renderer.ctx.device)
