@@ -25,6 +25,7 @@ HTC_RECIPE_EU_GRADIENT = 4
 HTC_RECIPE_CUSTOM = 100
 HTC_ERR_BUDGET = -5
 HTC_FLAG_JITTER_YX = 1
+HTC_FLAG_NO_SORT = 2
 
 STAT_SAMPLES, STAT_HOPS, STAT_OBJECT_TESTS, STAT_HITS = 0, 1, 2, 3
 

@@ -82,6 +82,8 @@ struct htc_program {
     void *wave_buf;            // two wavefront queues (WAVE_SLOT_BYTES per slot each), grown on demand
     size_t wave_slots;         // slots per queue
     uint32_t *d_wave_ctr;      // 2 counters per hop depth
+    void *sort_buf;            // coherence sort of the hyperbolic queues (SortBuf), grown with them
+    size_t sort_slots;
     int double_support;        // scene bytes in the double_support layout, narrowed before rendering
     uint8_t *narrow_buf;       // the narrowed (f32 layout) scene, grown on demand
     size_t narrow_bytes;
@@ -513,6 +515,7 @@ struct WaveQueue {      // ray state, structure of arrays (one float4 load / sto
     float4 *t;          // intensity xyz, RNG state (bits) in w
     float4 *e;          // emission xyz, pixel index (bits) in w
     uint32_t *h;        // previous hit hash
+    const uint32_t *o;  // read order: lane i of a hop takes slot o[i] (NULL: slot i)
 };
 constexpr size_t WAVE_SLOT_BYTES = 4 * sizeof(float4) + sizeof(uint32_t);
 
@@ -544,6 +547,7 @@ __host__ __device__ inline WaveQueue wave_at(const WaveQueue &q, uint64_t off) {
     r.t = q.t ? q.t + off : nullptr;
     r.e = q.e ? q.e + off : nullptr;
     r.h = q.h ? q.h + off : nullptr;
+    r.o = q.o ? q.o + off : nullptr;
     return r;
 }
 
@@ -576,13 +580,14 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
             rng = seeds[i];
             ray = camera<R>(s, px, py, size, rng, flags);
         } else {
-            ray = path_load<R>(in.p[i], in.v[i]);
-            const float4 t = in.t[i], e = in.e[i];
+            const uint32_t k = in.o ? in.o[i] : i;
+            ray = path_load<R>(in.p[k], in.v[k]);
+            const float4 t = in.t[k], e = in.e[k];
             intensity.x = t.x; intensity.y = t.y; intensity.z = t.z;
             rng = __float_as_uint(t.w);
             emission.x = e.x; emission.y = e.y; emission.z = e.z;
             pixel = __float_as_uint(e.w);
-            prev_hash = in.h[i];
+            prev_hash = in.h[k];
         }
         bool hit;
         st.hops += 1;
@@ -641,6 +646,197 @@ __global__ void __launch_bounds__(128, HT_WAVE_MINB) render_wave(
         wave_chunk<R, FH>(s, base, n, FH == 1, last, W, H, flags, canvas, seeds, in, out, &ctr[1], st);
     }
     flush_lane_stats(stats, st);
+}
+
+// ============================================================================ coherence sort
+// Between two hop depths of a hyperbolic pass the new queue gets a read order in which
+// neighbouring slots hold rays that leave in similar directions from nearby points: from
+// hop depth 2 on, rays start all over the scene, and the lanes of a warp otherwise carry
+// unrelated candidate lists through the per-lane loops of the scan (ray-aware bound, exact
+// tests), which then run with about 18 of 32 lanes active. Each path keeps its own state,
+// so the order changes no result, only which paths share a warp.
+//
+// The order is a counting sort on a 16-bit key: direction cell (the cube face the
+// direction points at, 4 x 4 cells per face: 96 cells) in the high bits, then a 3-bit
+// cell per axis of the ray start (x, y, log z) over mean +- 2 sigma of the queue itself,
+// interleaved (Morton order). Four launches per hop depth, all sized for the largest queue
+// and reading its length on the device: position sums (k_sort_stats), keys and their
+// histogram (k_sort_keys), the exclusive scan of the histogram (k_sort_scan, which also
+// clears the sums and the histogram for the next use) and the scatter of slot indices to
+// their sorted positions (k_sort_scatter). Ties within a key land in atomic order.
+constexpr uint32_t SORT_BINS = 1u << 16;
+constexpr uint32_t SORT_THREADS = 256;
+struct SortBuf {
+    double *acc;        // sum and sum of squares of x, y, log z (6 words)
+    uint32_t *hist;     // SORT_BINS counts
+    uint32_t *cursor;   // SORT_BINS next positions
+    uint16_t *key;      // per slot
+    uint32_t *perm;     // per sorted position: the slot
+};
+constexpr size_t sort_bytes(size_t slots) {
+    return 64 + 2 * sizeof(uint32_t) * SORT_BINS + ((sizeof(uint16_t) * slots + 15) & ~(size_t)15) +
+           sizeof(uint32_t) * slots;
+}
+static SortBuf sort_buf_at(void *base, size_t slots) {
+    SortBuf b;
+    uint8_t *c = reinterpret_cast<uint8_t *>(base);
+    b.acc = reinterpret_cast<double *>(c);
+    b.hist = reinterpret_cast<uint32_t *>(c + 64);
+    b.cursor = b.hist + SORT_BINS;
+    b.key = reinterpret_cast<uint16_t *>(b.cursor + SORT_BINS);
+    b.perm = reinterpret_cast<uint32_t *>(c + 64 + 2 * sizeof(uint32_t) * SORT_BINS +
+                                          ((sizeof(uint16_t) * slots + 15) & ~(size_t)15));
+    return b;
+}
+
+__device__ __forceinline__ float sort_logz(float z) { return z > 0.0f ? __logf(z) : 0.0f; }
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_stats(const float4 *__restrict__ p, const uint32_t *count,
+                                                            double *acc) {
+    const uint32_t n = *count;
+    float s[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t i = blockIdx.x * SORT_THREADS + threadIdx.x; i < n; i += gridDim.x * SORT_THREADS) {
+        const float4 q = p[i];
+        const float l = sort_logz(q.z);
+        s[0] += q.x; s[1] += q.x * q.x;
+        s[2] += q.y; s[3] += q.y * q.y;
+        s[4] += l;   s[5] += l * l;
+    }
+    __shared__ double part[SORT_THREADS / 32][6];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double d = s[k];
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) part[warp][k] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double d = 0.0;
+        for (uint32_t w = 0; w < SORT_THREADS / 32; ++w) d += part[w][threadIdx.x];
+        if (d != 0.0) atomicAdd(&acc[threadIdx.x], d);
+    }
+}
+
+__device__ __forceinline__ uint32_t sort_axis_cell(float u, float lo, float scale) {
+    return (uint32_t)fminf(fmaxf((u - lo) * scale, 0.0f), 7.0f);   // NaN -> 0
+}
+__device__ __forceinline__ uint32_t spread3(uint32_t c) {   // bits b2 b1 b0 -> b2 0 0 b1 0 0 b0
+    return (c & 1u) | ((c & 2u) << 2) | ((c & 4u) << 4);
+}
+__device__ __forceinline__ uint32_t sort_dir_cell(float4 v) {
+    const float ax = fabsf(v.x), ay = fabsf(v.y), az = fabsf(v.z);
+    uint32_t face;
+    float m, a, b;
+    if (ax >= ay && ax >= az) { face = v.x > 0.0f ? 1u : 0u; m = ax; a = v.y; b = v.z; }
+    else if (ay >= az)        { face = v.y > 0.0f ? 3u : 2u; m = ay; a = v.z; b = v.x; }
+    else                      { face = v.z > 0.0f ? 5u : 4u; m = az; a = v.x; b = v.y; }
+    const float r = m > 0.0f ? __frcp_rn(m) : 0.0f;
+    const uint32_t ia = (uint32_t)fminf(fmaxf((a * r + 1.0f) * 2.0f, 0.0f), 3.0f);
+    const uint32_t ib = (uint32_t)fminf(fmaxf((b * r + 1.0f) * 2.0f, 0.0f), 3.0f);
+    return face * 16u + ia * 4u + ib;
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_keys(const float4 *__restrict__ p, const float4 *__restrict__ v,
+                                                           const uint32_t *count, const double *acc,
+                                                           uint16_t *__restrict__ key, uint32_t *hist) {
+    const uint32_t n = *count;
+    if (n == 0) return;
+    float lo[3], scale[3];
+    const double inv_n = 1.0 / (double)n;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double mean = acc[2 * a] * inv_n;
+        const double var = fmax(acc[2 * a + 1] * inv_n - mean * mean, 0.0);
+        const double sd = sqrt(var);
+        lo[a] = (float)(mean - 2.0 * sd);
+        scale[a] = sd > 0.0 ? (float)(8.0 / (4.0 * sd)) : 0.0f;
+    }
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (SORT_THREADS / 32);
+    for (uint32_t base = (blockIdx.x * (SORT_THREADS / 32) + (threadIdx.x >> 5)) * 32u; base < n; base += warps * 32u) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        uint32_t k = 0x10000u + lane;   // lanes past the end group alone
+        if (valid) {
+            const float4 q = p[i];
+            const uint32_t cx = sort_axis_cell(q.x, lo[0], scale[0]);
+            const uint32_t cy = sort_axis_cell(q.y, lo[1], scale[1]);
+            const uint32_t cz = sort_axis_cell(sort_logz(q.z), lo[2], scale[2]);
+            k = sort_dir_cell(v[i]) * 512u + (spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2));
+            key[i] = (uint16_t)k;
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, k);
+        if (valid && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&hist[k], (uint32_t)__popc(grp));
+    }
+}
+
+// One block: exclusive scan of the histogram into the cursors; clears the histogram and
+// the position sums for the next hop depth. Warp w owns bins [2048 w, 2048 w + 2048), read
+// as 16 coalesced rows of 32 x 16 bytes (the scan is latency-bound: one SM, 256 KB).
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *hist, uint32_t *cursor, double *acc) {
+    constexpr uint32_t ROWS = SORT_BINS / 1024 / 4;   // rows of 32 uint4 per warp
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    uint4 *h4 = reinterpret_cast<uint4 *>(hist) + (size_t)warp * ROWS * 32 + lane;
+    uint4 *c4 = reinterpret_cast<uint4 *>(cursor) + (size_t)warp * ROWS * 32 + lane;
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < ROWS; ++j) {
+        const uint4 a = h4[32 * j];
+        sum += (a.x + a.y) + (a.z + a.w);
+    }
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);   // the warp's total
+    __shared__ uint32_t wsum[32];
+    if (lane == 0) wsum[warp] = sum;
+    __syncthreads();
+    if (warp == 0) {   // exclusive scan of the warp totals
+        const uint32_t w0 = wsum[lane];
+        uint32_t w = w0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        wsum[lane] = w - w0;
+    }
+    __syncthreads();
+    uint32_t run = wsum[warp];
+#pragma unroll
+    for (uint32_t j = 0; j < ROWS; ++j) {
+        const uint4 a = h4[32 * j];
+        const uint32_t s4 = (a.x + a.y) + (a.z + a.w);
+        uint32_t x = s4;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        uint4 r;
+        r.x = run + x - s4;
+        r.y = r.x + a.x;
+        r.z = r.y + a.y;
+        r.w = r.z + a.z;
+        c4[32 * j] = r;
+        h4[32 * j] = make_uint4(0u, 0u, 0u, 0u);
+        run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (t < 6) acc[t] = 0.0;
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint16_t *__restrict__ key, const uint32_t *count,
+                                                              uint32_t *cursor, uint32_t *__restrict__ perm) {
+    const uint32_t n = *count;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (SORT_THREADS / 32);
+    for (uint32_t base = (blockIdx.x * (SORT_THREADS / 32) + (threadIdx.x >> 5)) * 32u; base < n; base += warps * 32u) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t k = valid ? (uint32_t)key[i] : 0x10000u + lane;
+        const uint32_t grp = __match_any_sync(0xffffffffu, k);
+        const int leader = __ffs(grp) - 1;
+        uint32_t at = 0;
+        if (valid && lane == (uint32_t)leader) at = atomicAdd(&cursor[k], (uint32_t)__popc(grp));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (valid) perm[at + __popc(grp & ((1u << lane) - 1u))] = i;
+    }
 }
 
 // ============================================================================ batch
@@ -1025,7 +1221,7 @@ int htc_program_create(int recipe, uint32_t light_hops, int address_width, int d
         return fail(HTC_ERR_UNSUPPORTED, "unknown scene recipe");
     if (light_hops == 0) return fail(HTC_ERR_INVALID, "light_hops must be positive");
     if (address_width != 32 && address_width != 64) return fail(HTC_ERR_INVALID, "address_width must be 32 or 64");
-    if (flags & ~HTC_FLAG_JITTER_YX) return fail(HTC_ERR_INVALID, "unknown program flags");
+    if (flags & ~(HTC_FLAG_JITTER_YX | HTC_FLAG_NO_SORT)) return fail(HTC_ERR_INVALID, "unknown program flags");
     if (double_support && recipe != HTC_RECIPE_HY && recipe != HTC_RECIPE_EU)
         return fail(HTC_ERR_UNSUPPORTED, "double_support scenes are served for HTC_RECIPE_HY and HTC_RECIPE_EU only");
     if (recipe == HTC_RECIPE_HY_TILED || recipe == HTC_RECIPE_EU_GRADIENT) {
@@ -1072,6 +1268,7 @@ void htc_program_destroy(htc_program *p) {
     if (p->d_queue) cudaFree(p->d_queue);
     if (p->wave_buf) cudaFree(p->wave_buf);
     if (p->d_wave_ctr) cudaFree(p->d_wave_ctr);
+    if (p->sort_buf) cudaFree(p->sort_buf);
     if (p->narrow_buf) cudaFree(p->narrow_buf);
     if (p->generic) generic_program_destroy(p->generic);
     delete p;
@@ -1237,6 +1434,17 @@ static int wave_reserve(htc_program *p, size_t slots) {
         HTC_CUDA(cudaMalloc(&p->d_wave_ctr, 2 * sizeof(uint32_t) * (size_t)p->hops));
     }
     slots = (slots + 63) & ~(size_t)63;   // keeps the second queue and every array 16-byte aligned
+    if (p->recipe == HTC_RECIPE_HY && !(p->flags & HTC_FLAG_NO_SORT) && p->sort_slots < slots) {
+        if (p->sort_buf) {
+            HTC_CUDA(cudaFree(p->sort_buf));
+            p->sort_buf = nullptr;
+            p->sort_slots = 0;
+        }
+        HTC_CUDA(cudaMalloc(&p->sort_buf, sort_bytes(slots)));
+        // sums and histogram start cleared; k_sort_scan clears them after each use
+        HTC_CUDA(cudaMemset(p->sort_buf, 0, 64 + sizeof(uint32_t) * SORT_BINS));
+        p->sort_slots = slots;
+    }
     if (p->wave_slots >= slots) return HTC_OK;
     if (p->wave_buf) {
         HTC_CUDA(cudaFree(p->wave_buf));
@@ -1256,6 +1464,7 @@ static WaveQueue wave_queue(htc_program *p, int which) {
     q.t = q.v + n;
     q.e = q.t + n;
     q.h = reinterpret_cast<uint32_t *>(q.e + n);
+    q.o = nullptr;
     return q;
 }
 template <int R>
@@ -1269,12 +1478,23 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
     const uint64_t needed = ((uint64_t)W * H + 127) / 128;
     if (blocks > needed) blocks = needed;
     const WaveQueue q[2] = {wave_queue(p, 0), wave_queue(p, 1)};
-    const WaveQueue none = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    const WaveQueue none = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const bool sorted = R == RECIPE_HY && p->sort_buf != nullptr && !(p->flags & HTC_FLAG_NO_SORT);
+    const SortBuf sb = sorted ? sort_buf_at(p->sort_buf, p->sort_slots) : SortBuf{};
+    const unsigned sort_blocks = (unsigned)std::min<uint64_t>((uint64_t)p->num_sms * 8u,
+                                                             ((uint64_t)W * H + SORT_THREADS - 1) / SORT_THREADS);
     for (uint32_t pass = 0; pass < passes; ++pass) {
         HTC_CUDA(cudaMemsetAsync(p->d_wave_ctr, 0, 2 * sizeof(uint32_t) * (size_t)p->hops, st));
         for (uint32_t h = 0; h < p->hops; ++h) {
-            const WaveQueue in = h == 0 ? none : q[(h - 1) & 1];
+            WaveQueue in = h == 0 ? none : q[(h - 1) & 1];
             const uint32_t *in_count = h == 0 ? nullptr : p->d_wave_ctr + 2 * (h - 1) + 1;
+            if (sorted && h > 0) {
+                k_sort_stats<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in_count, sb.acc);
+                k_sort_keys<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in.v, in_count, sb.acc, sb.key, sb.hist);
+                k_sort_scan<<<1, 1024, 0, st>>>(sb.hist, sb.cursor, sb.acc);
+                k_sort_scatter<<<sort_blocks, SORT_THREADS, 0, st>>>(sb.key, in_count, sb.cursor, sb.perm);
+                in.o = sb.perm;
+            }
             (h == 0 ? render_wave<R, 1> : render_wave<R, 2>)<<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
                                                                p->hops, h, p->flags, cv, seeds, stats, p->d_err, in,
                                                                in_count, q[h & 1], p->d_wave_ctr + 2 * h);
@@ -1494,6 +1714,7 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
         q[k].t = q[k].v + n;
         q[k].e = q[k].t + n;
         q[k].h = reinterpret_cast<uint32_t *>(q[k].e + n);
+        q[k].o = nullptr;
     }
     unsigned blocks_any = 0, blocks_hy = 0, blocks_eu = 0;
     int rc = HT_BATCH_SPLIT ? batch_wave_blocks<RECIPE_HY>(b, smem, &blocks_hy) : batch_wave_blocks<0>(b, smem, &blocks_any);

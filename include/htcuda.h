@@ -60,6 +60,10 @@ extern "C" {
                                   evaluates random_uniform2's arguments in the reference's
                                   host build (kernel/ocl/random.cc:15-20); the default is
                                   the OpenCL order (first draw -> x). */
+#define HTC_FLAG_NO_SORT 2u    /* hyperbolic wavefronts (htc_render_wavefront / _passes) take
+                                  each hop depth's paths in queue order instead of sorting them
+                                  by direction and start cell first; the results are the same
+                                  bits either way (htc_program_create only). */
 
 /* Render statistics written by the entry points that take a `stats` pointer (device
  * buffer of HTC_STAT_COUNT x uint64, accumulated with atomics; zero it before the launch). */

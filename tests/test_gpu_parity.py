@@ -119,16 +119,18 @@ def test_device_seeds_equal_host_seeds(built, W, H, seed):
     assert np.array_equal(canvas.seeds.cpu().numpy().view(np.uint32), S.pixel_seeds(seed, W * H))
 
 
+@pytest.mark.parametrize("sort", [True, False])
 @pytest.mark.parametrize("cfg,W,H,passes", [("config0", 160, 120, 5), ("config1", 200, 150, 3),
                                            ("config2", 480, 270, 2), ("config1", 33, 7, 4),
                                            ("config1", 1, 1, 3), ("config0", 1, 37, 2)])
-def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes):
+def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes, sort):
     """Hop-depth wavefronts over ray-state queues == P plain launches, bit for bit, with the
-    same statistics (samples, hops, hits, exact tests)."""
+    same statistics (samples, hops, hits, exact tests); hyperbolic queues with and without the
+    coherence sort between hop depths."""
     wl = getattr(S, cfg)()
     ctx = P.Context(0)
     buf = P.EntityBuffer(ctx, wl.scene)
-    r = P.Render(ctx, wl.scene.recipe, wl.scene.hops)
+    r = P.Render(ctx, wl.scene.recipe, wl.scene.hops, 0 if sort else _lib.HTC_FLAG_NO_SORT)
     out = []
     for wave in (False, True):
         canvas = P.Canvas(ctx, (W, H), global_seed=wl.global_seed)
@@ -145,6 +147,34 @@ def test_wavefront_equals_repeated_plain(built, cfg, W, H, passes):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][2], out[1][2])
     assert out[1][2][_lib.STAT_SAMPLES] == W * H * passes
+
+
+@pytest.mark.parametrize("seed", [None, 3, 4])
+def test_sorted_wavefront_full_frame(built, seed):
+    """The coherence sort at full size: one pass of the 1920x1080 hyperbolic frame (and of
+    random hyperbolic scenes) with and without it gives the same canvas, seeds and statistics,
+    so every queued path ran exactly once, whatever order the sort gave it."""
+    if seed is None:
+        wl = S.config2()
+        scene, W, H, gs = wl.scene, wl.width, wl.height, wl.global_seed
+    else:
+        rng = np.random.default_rng(seed)
+        scene = S.hyperbolic_scene(30 + 50 * seed, 60, 6.0, 8, 700 + seed, camera=S.random_moebius(rng, 1.0))
+        W, H, gs = 1280, 720, seed
+    ctx = P.Context(0)
+    buf = P.EntityBuffer(ctx, scene)
+    out = []
+    for flags in (0, _lib.HTC_FLAG_NO_SORT):
+        r = P.Render(ctx, scene.recipe, scene.hops, flags)
+        canvas = P.Canvas(ctx, (W, H), global_seed=gs)
+        stats = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+        r.render_wavefront(buf, canvas, 1, stats=stats)
+        torch.cuda.synchronize()
+        out.append((canvas.image.view(torch.int32).cpu(), canvas.seeds.cpu(), stats.cpu()))
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
+    assert torch.equal(out[0][2], out[1][2])
+    assert int(out[0][2][_lib.STAT_SAMPLES]) == W * H
 
 
 def test_wavefront_single_hop_and_reuse(built):
