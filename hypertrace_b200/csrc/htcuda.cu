@@ -658,66 +658,50 @@ __global__ void __launch_bounds__(128, HT_WAVE_MINB) render_wave(
 //
 // The order is a counting sort on a 16-bit key: direction cell (the cube face the
 // direction points at, 4 x 4 cells per face: 96 cells) in the high bits, then a 3-bit
-// cell per axis of the ray start (x, y, log z) over mean +- 2 sigma of the queue itself,
-// interleaved (Morton order). Four launches per hop depth, all sized for the largest queue
-// and reading its length on the device: position sums (k_sort_stats), keys and their
-// histogram (k_sort_keys), the exclusive scan of the histogram (k_sort_scan, which also
-// clears the sums and the histogram for the next use) and the scatter of slot indices to
-// their sorted positions (k_sort_scatter). Ties within a key land in atomic order.
+// cell per axis of the ray start (x, y, log z) over mean +- 2 sigma of that hop depth's
+// queue in the previous pass, interleaved (Morton order); until a depth has been seen once,
+// its cells are all zero and the sort goes by direction alone. Four launches per hop depth,
+// sized for the largest queue and reading its length on the device: keys, their histogram
+// and the position sums (k_sort_keys); the histogram's block totals (k_sort_scan_blocks);
+// the exclusive scan into cursors, which also clears the histogram and turns the sums into
+// the depth's next cells (k_sort_scan); the scatter of slot indices to their sorted
+// positions (k_sort_scatter). Ties within a key land in atomic order. The work stays out of
+// the hop kernel: that kernel is bound by instruction fetch as much as by issue, and the
+// same steps inlined at its append site made every hop launch slower than these launches.
 constexpr uint32_t SORT_BINS = 1u << 16;
 constexpr uint32_t SORT_THREADS = 256;
+constexpr uint32_t SORT_SCAN_BLOCKS = SORT_BINS / (4 * SORT_THREADS);   // 64: one uint4 of bins per thread
+constexpr uint32_t SORT_DEPTH_WORDS = 8;   // per hop depth: 6 sums (double) / 6 cell bounds (float)
 struct SortBuf {
-    double *acc;        // sum and sum of squares of x, y, log z (6 words)
+    double *acc;        // per hop depth: sum and sum of squares of x, y, log z
+    float *cut;         // per hop depth: lower bound of x, y, log z, then cells per unit
     uint32_t *hist;     // SORT_BINS counts
+    uint32_t *bsum;     // SORT_SCAN_BLOCKS block totals of the histogram
     uint32_t *cursor;   // SORT_BINS next positions
     uint16_t *key;      // per slot
     uint32_t *perm;     // per sorted position: the slot
 };
-constexpr size_t sort_bytes(size_t slots) {
-    return 64 + 2 * sizeof(uint32_t) * SORT_BINS + ((sizeof(uint16_t) * slots + 15) & ~(size_t)15) +
-           sizeof(uint32_t) * slots;
+constexpr size_t sort_head_bytes(uint32_t hops) {   // acc, cut, hist: cleared at allocation
+    return (size_t)hops * SORT_DEPTH_WORDS * (sizeof(double) + sizeof(float)) + sizeof(uint32_t) * SORT_BINS;
 }
-static SortBuf sort_buf_at(void *base, size_t slots) {
+constexpr size_t sort_bytes(size_t slots, uint32_t hops) {
+    return sort_head_bytes(hops) + sizeof(uint32_t) * (SORT_SCAN_BLOCKS + SORT_BINS) +
+           ((sizeof(uint16_t) * slots + 15) & ~(size_t)15) + sizeof(uint32_t) * slots;
+}
+static SortBuf sort_buf_at(void *base, size_t slots, uint32_t hops) {
     SortBuf b;
-    uint8_t *c = reinterpret_cast<uint8_t *>(base);
-    b.acc = reinterpret_cast<double *>(c);
-    b.hist = reinterpret_cast<uint32_t *>(c + 64);
-    b.cursor = b.hist + SORT_BINS;
+    b.acc = reinterpret_cast<double *>(base);
+    b.cut = reinterpret_cast<float *>(b.acc + (size_t)hops * SORT_DEPTH_WORDS);
+    b.hist = reinterpret_cast<uint32_t *>(b.cut + (size_t)hops * SORT_DEPTH_WORDS);
+    b.bsum = b.hist + SORT_BINS;
+    b.cursor = b.bsum + SORT_SCAN_BLOCKS;
     b.key = reinterpret_cast<uint16_t *>(b.cursor + SORT_BINS);
-    b.perm = reinterpret_cast<uint32_t *>(c + 64 + 2 * sizeof(uint32_t) * SORT_BINS +
+    b.perm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(b.key) +
                                           ((sizeof(uint16_t) * slots + 15) & ~(size_t)15));
     return b;
 }
 
 __device__ __forceinline__ float sort_logz(float z) { return z > 0.0f ? __logf(z) : 0.0f; }
-
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_stats(const float4 *__restrict__ p, const uint32_t *count,
-                                                            double *acc) {
-    const uint32_t n = *count;
-    float s[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    for (uint32_t i = blockIdx.x * SORT_THREADS + threadIdx.x; i < n; i += gridDim.x * SORT_THREADS) {
-        const float4 q = p[i];
-        const float l = sort_logz(q.z);
-        s[0] += q.x; s[1] += q.x * q.x;
-        s[2] += q.y; s[3] += q.y * q.y;
-        s[4] += l;   s[5] += l * l;
-    }
-    __shared__ double part[SORT_THREADS / 32][6];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        double d = s[k];
-        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-        if (lane == 0) part[warp][k] = d;
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        double d = 0.0;
-        for (uint32_t w = 0; w < SORT_THREADS / 32; ++w) d += part[w][threadIdx.x];
-        if (d != 0.0) atomicAdd(&acc[threadIdx.x], d);
-    }
-}
-
 __device__ __forceinline__ uint32_t sort_axis_cell(float u, float lo, float scale) {
     return (uint32_t)fminf(fmaxf((u - lo) * scale, 0.0f), 7.0f);   // NaN -> 0
 }
@@ -734,91 +718,116 @@ __device__ __forceinline__ uint32_t sort_dir_cell(float4 v) {
     const float r = m > 0.0f ? __frcp_rn(m) : 0.0f;
     const uint32_t ia = (uint32_t)fminf(fmaxf((a * r + 1.0f) * 2.0f, 0.0f), 3.0f);
     const uint32_t ib = (uint32_t)fminf(fmaxf((b * r + 1.0f) * 2.0f, 0.0f), 3.0f);
-    return face * 16u + ia * 4u + ib;
+    return face * 16u + ia * 4u + ib;   // < 96
 }
 
+// Keys (< 96 * 512 = 49152) of the `count` queued paths with the depth's cells `cut`, their
+// histogram (lanes of a warp with equal keys add once) and the position sums into `acc`.
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_keys(const float4 *__restrict__ p, const float4 *__restrict__ v,
-                                                           const uint32_t *count, const double *acc,
+                                                           const uint32_t *count, const float *cut, double *acc,
                                                            uint16_t *__restrict__ key, uint32_t *hist) {
     const uint32_t n = *count;
     if (n == 0) return;
-    float lo[3], scale[3];
-    const double inv_n = 1.0 / (double)n;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double mean = acc[2 * a] * inv_n;
-        const double var = fmax(acc[2 * a + 1] * inv_n - mean * mean, 0.0);
-        const double sd = sqrt(var);
-        lo[a] = (float)(mean - 2.0 * sd);
-        scale[a] = sd > 0.0 ? (float)(8.0 / (4.0 * sd)) : 0.0f;
-    }
+    const float lo0 = cut[0], lo1 = cut[1], lo2 = cut[2], sc0 = cut[3], sc1 = cut[4], sc2 = cut[5];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (SORT_THREADS / 32);
+    float s[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     for (uint32_t base = (blockIdx.x * (SORT_THREADS / 32) + (threadIdx.x >> 5)) * 32u; base < n; base += warps * 32u) {
         const uint32_t i = base + lane;
         const bool valid = i < n;
         uint32_t k = 0x10000u + lane;   // lanes past the end group alone
         if (valid) {
             const float4 q = p[i];
-            const uint32_t cx = sort_axis_cell(q.x, lo[0], scale[0]);
-            const uint32_t cy = sort_axis_cell(q.y, lo[1], scale[1]);
-            const uint32_t cz = sort_axis_cell(sort_logz(q.z), lo[2], scale[2]);
+            const float l = sort_logz(q.z);
+            s[0] += q.x; s[1] += q.x * q.x;
+            s[2] += q.y; s[3] += q.y * q.y;
+            s[4] += l;   s[5] += l * l;
+            const uint32_t cx = sort_axis_cell(q.x, lo0, sc0);
+            const uint32_t cy = sort_axis_cell(q.y, lo1, sc1);
+            const uint32_t cz = sort_axis_cell(l, lo2, sc2);
             k = sort_dir_cell(v[i]) * 512u + (spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2));
             key[i] = (uint16_t)k;
         }
         const uint32_t grp = __match_any_sync(0xffffffffu, k);
         if (valid && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&hist[k], (uint32_t)__popc(grp));
     }
+    __shared__ double part[SORT_THREADS / 32][6];
+    const uint32_t warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double d = s[q];
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) part[warp][q] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double d = 0.0;
+        for (uint32_t w = 0; w < SORT_THREADS / 32; ++w) d += part[w][threadIdx.x];
+        if (d != 0.0) atomicAdd(&acc[threadIdx.x], d);
+    }
 }
 
-// One block: exclusive scan of the histogram into the cursors; clears the histogram and
-// the position sums for the next hop depth. Warp w owns bins [2048 w, 2048 w + 2048), read
-// as 16 coalesced rows of 32 x 16 bytes (the scan is latency-bound: one SM, 256 KB).
-__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *hist, uint32_t *cursor, double *acc) {
-    constexpr uint32_t ROWS = SORT_BINS / 1024 / 4;   // rows of 32 uint4 per warp
+// Block totals of the histogram: block b sums bins [1024 b, 1024 b + 1024), one coalesced
+// 16-byte load per thread.
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scan_blocks(const uint32_t *hist, uint32_t *bsum) {
+    const uint4 a = reinterpret_cast<const uint4 *>(hist)[blockIdx.x * SORT_THREADS + threadIdx.x];
+    uint32_t s = (a.x + a.y) + (a.z + a.w);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ uint32_t w[SORT_THREADS / 32];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) w[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (uint32_t k = 0; k < SORT_THREADS / 32; ++k) t += w[k];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the histogram into the cursors (block b: bins [1024 b, 1024 b + 1024),
+// offset by the totals of the blocks before it), clearing the histogram. Block 0 also turns
+// the depth's position sums over its `count` paths into the cells the next pass keys it
+// with (mean - 2 sigma, 8 cells over 4 sigma per axis) and clears the sums.
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scan(uint32_t *hist, const uint32_t *bsum, uint32_t *cursor,
+                                                           double *acc, float *cut, const uint32_t *count) {
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    uint4 *h4 = reinterpret_cast<uint4 *>(hist) + (size_t)warp * ROWS * 32 + lane;
-    uint4 *c4 = reinterpret_cast<uint4 *>(cursor) + (size_t)warp * ROWS * 32 + lane;
-    uint32_t sum = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < ROWS; ++j) {
-        const uint4 a = h4[32 * j];
-        sum += (a.x + a.y) + (a.z + a.w);
+    __shared__ uint32_t w[SORT_THREADS / 32];
+    __shared__ uint32_t base_s[2];
+    if (warp < 2) {   // the blocks before this one (SORT_SCAN_BLOCKS = 64 totals)
+        uint32_t b = t < blockIdx.x ? bsum[t] : 0u;
+        for (int o = 16; o; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+        if (lane == 0) base_s[warp] = b;
     }
-    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);   // the warp's total
-    __shared__ uint32_t wsum[32];
-    if (lane == 0) wsum[warp] = sum;
+    uint4 *h4 = reinterpret_cast<uint4 *>(hist) + blockIdx.x * SORT_THREADS + t;
+    const uint4 a = *h4;
+    const uint32_t s4 = (a.x + a.y) + (a.z + a.w);
+    uint32_t x = s4;   // inclusive scan within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) w[warp] = x;
     __syncthreads();
-    if (warp == 0) {   // exclusive scan of the warp totals
-        const uint32_t w0 = wsum[lane];
-        uint32_t w = w0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= (uint32_t)o) w += y;
+    uint32_t run = base_s[0] + base_s[1] + x - s4;
+    for (uint32_t k = 0; k < warp; ++k) run += w[k];
+    uint4 r;
+    r.x = run;
+    r.y = r.x + a.x;
+    r.z = r.y + a.y;
+    r.w = r.z + a.z;
+    reinterpret_cast<uint4 *>(cursor)[blockIdx.x * SORT_THREADS + t] = r;
+    *h4 = make_uint4(0u, 0u, 0u, 0u);
+    if (blockIdx.x == 0 && t < 3) {
+        const uint32_t n = *count;
+        if (n) {
+            const double mean = acc[2 * t] / (double)n;
+            const double sd = sqrt(fmax(acc[2 * t + 1] / (double)n - mean * mean, 0.0));
+            cut[t] = (float)(mean - 2.0 * sd);
+            cut[3 + t] = sd > 0.0 ? (float)(2.0 / sd) : 0.0f;   // 8 cells over 4 sigma
         }
-        wsum[lane] = w - w0;
+        acc[2 * t] = 0.0;
+        acc[2 * t + 1] = 0.0;
     }
-    __syncthreads();
-    uint32_t run = wsum[warp];
-#pragma unroll
-    for (uint32_t j = 0; j < ROWS; ++j) {
-        const uint4 a = h4[32 * j];
-        const uint32_t s4 = (a.x + a.y) + (a.z + a.w);
-        uint32_t x = s4;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= (uint32_t)o) x += y;
-        }
-        uint4 r;
-        r.x = run + x - s4;
-        r.y = r.x + a.x;
-        r.z = r.y + a.y;
-        r.w = r.z + a.z;
-        c4[32 * j] = r;
-        h4[32 * j] = make_uint4(0u, 0u, 0u, 0u);
-        run += __shfl_sync(0xffffffffu, x, 31);
-    }
-    if (t < 6) acc[t] = 0.0;
 }
 
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint16_t *__restrict__ key, const uint32_t *count,
@@ -1440,9 +1449,9 @@ static int wave_reserve(htc_program *p, size_t slots) {
             p->sort_buf = nullptr;
             p->sort_slots = 0;
         }
-        HTC_CUDA(cudaMalloc(&p->sort_buf, sort_bytes(slots)));
-        // sums and histogram start cleared; k_sort_scan clears them after each use
-        HTC_CUDA(cudaMemset(p->sort_buf, 0, 64 + sizeof(uint32_t) * SORT_BINS));
+        HTC_CUDA(cudaMalloc(&p->sort_buf, sort_bytes(slots, p->hops)));
+        // sums, cells and histogram start cleared; k_sort_scan clears sums and histogram after each use
+        HTC_CUDA(cudaMemset(p->sort_buf, 0, sort_head_bytes(p->hops)));
         p->sort_slots = slots;
     }
     if (p->wave_slots >= slots) return HTC_OK;
@@ -1480,7 +1489,7 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
     const WaveQueue q[2] = {wave_queue(p, 0), wave_queue(p, 1)};
     const WaveQueue none = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     const bool sorted = R == RECIPE_HY && p->sort_buf != nullptr && !(p->flags & HTC_FLAG_NO_SORT);
-    const SortBuf sb = sorted ? sort_buf_at(p->sort_buf, p->sort_slots) : SortBuf{};
+    const SortBuf sb = sorted ? sort_buf_at(p->sort_buf, p->sort_slots, p->hops) : SortBuf{};
     const unsigned sort_blocks = (unsigned)std::min<uint64_t>((uint64_t)p->num_sms * 8u,
                                                              ((uint64_t)W * H + SORT_THREADS - 1) / SORT_THREADS);
     for (uint32_t pass = 0; pass < passes; ++pass) {
@@ -1489,9 +1498,11 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
             WaveQueue in = h == 0 ? none : q[(h - 1) & 1];
             const uint32_t *in_count = h == 0 ? nullptr : p->d_wave_ctr + 2 * (h - 1) + 1;
             if (sorted && h > 0) {
-                k_sort_stats<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in_count, sb.acc);
-                k_sort_keys<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in.v, in_count, sb.acc, sb.key, sb.hist);
-                k_sort_scan<<<1, 1024, 0, st>>>(sb.hist, sb.cursor, sb.acc);
+                double *acc = sb.acc + (size_t)h * SORT_DEPTH_WORDS;
+                float *cut = sb.cut + (size_t)h * SORT_DEPTH_WORDS;
+                k_sort_keys<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in.v, in_count, cut, acc, sb.key, sb.hist);
+                k_sort_scan_blocks<<<SORT_SCAN_BLOCKS, SORT_THREADS, 0, st>>>(sb.hist, sb.bsum);
+                k_sort_scan<<<SORT_SCAN_BLOCKS, SORT_THREADS, 0, st>>>(sb.hist, sb.bsum, sb.cursor, acc, cut, in_count);
                 k_sort_scatter<<<sort_blocks, SORT_THREADS, 0, st>>>(sb.key, in_count, sb.cursor, sb.perm);
                 in.o = sb.perm;
             }
