@@ -53,8 +53,8 @@ UNIT = "Msamples/s"
 # instructions issued; DRAM bytes are read + written. Frozen from that capture (the summary with
 # the command is profiles/render_wave_hy1080p_200obj.md): re-capture after a kernel change.
 FP32_OPS_PER_HOP = 6051.9       # 59.37e9 per pass over 9.81e6 path-hops
-WARP_INSTR_PER_HOP = 460.97     # 4.523e9 per pass
-DRAM_BYTES_PER_HOP = 104.42     # 1.024e9 per pass
+WARP_INSTR_PER_HOP = 360.76     # 3.539e9 per pass
+DRAM_BYTES_PER_HOP = 157.22     # 1.542e9 per pass
 # The reference's own FP32 count per hop for comparison: every object's detect maps the ray in
 # and out (two ray maps of 256 operations, object/mapped.inl:32,34, plus the shape test), i.e.
 # 527 per object and hop. Distance culling skips 98 % of those tests, so this count can exceed
@@ -360,8 +360,11 @@ def main():
     value = all_samples / max_s / 1e6
 
     # roofline of render_wave (one launch per hop depth, `passes * hops` launches per step):
-    # measured operations per path-hop x this run's path-hops, over the device time
+    # measured operations per path-hop x this run's path-hops, over the device time of the
+    # step, which also holds the coherence sort between hop depths (4 launches per depth of a
+    # hyperbolic pass after the first)
     launches = args.steps * args.passes * sc.hops
+    sort_launches = args.steps * args.passes * (sc.hops - 1) * 4 if sc.recipe == _lib.HTC_RECIPE_HY else 0
     per_launch_s = dev_s / launches
     achieved = FP32_OPS_PER_HOP * hops / dev_s / 1e12 if FP32_OPS_PER_HOP else None
     ref_tflops = tests * REF_OPS_PER_OBJECT_TEST / dev_s / 1e12
@@ -469,8 +472,9 @@ def main():
                          "frac": achieved / fp32_peak_tflops if achieved and fp32_peak_tflops else None,
                          "traffic": DRAM_BYTES_PER_HOP * hops / launches if DRAM_BYTES_PER_HOP else None,
                          "source": "FP32 operations and DRAM bytes per path-hop: constants from one ncu "
-                                   "capture of a pass's 8 launches (ffma x2 + fadd + fmul, packed forms x2), "
-                                   "times this run's path-hops; traffic per launch",
+                                   "capture of a pass's 8 render_wave launches (ffma x2 + fadd + fmul, packed "
+                                   "forms x2), times this run's path-hops, over the step's device time (the "
+                                   "sort launches between hop depths included); traffic per render_wave launch",
                          "peak_source": "measured FFMA probe (htc_fp32_probe) on this GPU in this run",
                          "issue": {"achieved_ginstr_per_s": WARP_INSTR_PER_HOP * hops / dev_s / 1e9
                                    if WARP_INSTR_PER_HOP else None,
@@ -491,7 +495,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": launches,
+            "gpu_launches": launches + sort_launches,
             "wall_s_timed": t_wall,
             "launch_ms": [round(x, 3) for x in launch_ms],
         }

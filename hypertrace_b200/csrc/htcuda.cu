@@ -61,6 +61,9 @@ thread_local std::string g_last_error;
 #define HT_PASSES_MODE 2
 #endif
 // Batched wavefronts: 1 = one launch per recipe for each (pass, hop depth), 0 = one launch for both.
+#ifndef HT_BATCH_SORT   // coherence sort of the batch's hyperbolic views (with HT_BATCH_SPLIT)
+#define HT_BATCH_SORT 1
+#endif
 #ifndef HT_BATCH_SPLIT
 #define HT_BATCH_SPLIT 1
 #endif
@@ -770,7 +773,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_keys(const float4 *__rest
 // Block totals of the histogram: block b sums bins [1024 b, 1024 b + 1024), one coalesced
 // 16-byte load per thread.
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scan_blocks(const uint32_t *hist, uint32_t *bsum) {
-    const uint4 a = reinterpret_cast<const uint4 *>(hist)[blockIdx.x * SORT_THREADS + threadIdx.x];
+    const uint4 a = reinterpret_cast<const uint4 *>(hist)[(size_t)blockIdx.x * SORT_THREADS + threadIdx.x];
     uint32_t s = (a.x + a.y) + (a.z + a.w);
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     __shared__ uint32_t w[SORT_THREADS / 32];
@@ -785,20 +788,23 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scan_blocks(const uint32_
 }
 
 // Exclusive scan of the histogram into the cursors (block b: bins [1024 b, 1024 b + 1024),
-// offset by the totals of the blocks before it), clearing the histogram. Block 0 also turns
-// the depth's position sums over its `count` paths into the cells the next pass keys it
-// with (mean - 2 sigma, 8 cells over 4 sigma per axis) and clears the sums.
+// offset by the totals of the blocks before it), clearing the histogram. With `seg_base`,
+// the histogram is cut into segments of `seg_bins` bins (a multiple of 1024), one per
+// view, and the cursor value at each segment's first bin is recorded there, so that
+// positions within a view's queue are cursor - seg_base. With `acc`, block 0 also turns the
+// depth's position sums over its `count` paths into the cells the next pass keys it with
+// (mean - 2 sigma, 8 cells over 4 sigma per axis) and clears the sums.
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scan(uint32_t *hist, const uint32_t *bsum, uint32_t *cursor,
-                                                           double *acc, float *cut, const uint32_t *count) {
+                                                           uint32_t seg_bins, uint32_t *seg_base, double *acc,
+                                                           float *cut, const uint32_t *count) {
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
     __shared__ uint32_t w[SORT_THREADS / 32];
-    __shared__ uint32_t base_s[2];
-    if (warp < 2) {   // the blocks before this one (SORT_SCAN_BLOCKS = 64 totals)
-        uint32_t b = t < blockIdx.x ? bsum[t] : 0u;
-        for (int o = 16; o; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
-        if (lane == 0) base_s[warp] = b;
-    }
-    uint4 *h4 = reinterpret_cast<uint4 *>(hist) + blockIdx.x * SORT_THREADS + t;
+    __shared__ uint32_t base_w[SORT_THREADS / 32];
+    uint32_t before = 0;   // the totals of the blocks before this one
+    for (uint32_t k = t; k < blockIdx.x; k += SORT_THREADS) before += bsum[k];
+    for (int o = 16; o; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+    if (lane == 0) base_w[warp] = before;
+    uint4 *h4 = reinterpret_cast<uint4 *>(hist) + (size_t)blockIdx.x * SORT_THREADS + t;
     const uint4 a = *h4;
     const uint32_t s4 = (a.x + a.y) + (a.z + a.w);
     uint32_t x = s4;   // inclusive scan within the warp
@@ -808,16 +814,18 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scan(uint32_t *hist, cons
     }
     if (lane == 31) w[warp] = x;
     __syncthreads();
-    uint32_t run = base_s[0] + base_s[1] + x - s4;
-    for (uint32_t k = 0; k < warp; ++k) run += w[k];
+    uint32_t run = x - s4;
+    for (uint32_t k = 0; k < SORT_THREADS / 32; ++k) run += base_w[k] + (k < warp ? w[k] : 0u);
     uint4 r;
     r.x = run;
     r.y = r.x + a.x;
     r.z = r.y + a.y;
     r.w = r.z + a.z;
-    reinterpret_cast<uint4 *>(cursor)[blockIdx.x * SORT_THREADS + t] = r;
+    const size_t bin = ((size_t)blockIdx.x * SORT_THREADS + t) * 4;
+    reinterpret_cast<uint4 *>(cursor)[(size_t)blockIdx.x * SORT_THREADS + t] = r;
     *h4 = make_uint4(0u, 0u, 0u, 0u);
-    if (blockIdx.x == 0 && t < 3) {
+    if (seg_base && bin % seg_bins == 0) seg_base[bin / seg_bins] = r.x;
+    if (acc && blockIdx.x == 0 && t < 3) {
         const uint32_t n = *count;
         if (n) {
             const double mean = acc[2 * t] / (double)n;
@@ -885,7 +893,7 @@ template <int RF, int FH>
 __global__ void __launch_bounds__(128, RF ? HT_WAVE_MINB : HT_PERSIST_MINB) render_batch_wave(
     const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
     uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
-    uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err) {
+    uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err, uint32_t n_sorted) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t s_hdr[2 + BLOCK_THREADS / 32];
     __shared__ uint32_t s_tile, s_next, s_total, s_tsize;
@@ -976,7 +984,12 @@ __global__ void __launch_bounds__(128, RF ? HT_WAVE_MINB : HT_PERSIST_MINB) rend
             __syncthreads();
         }
         if (!s_staged_ok) continue;
-        const WaveQueue vin = wave_at(in, v.qoff + first), vout = wave_at(out, v.qoff);
+        // the first n_sorted views of `order` read a tile's paths through their sorted order
+        // (view-relative slots), the others in queue order
+        const bool sorted = in.o != nullptr && lo < n_sorted;
+        WaveQueue vin = wave_at(in, sorted ? v.qoff : v.qoff + first);
+        vin.o = sorted ? in.o + v.qoff + first : nullptr;
+        const WaveQueue vout = wave_at(out, v.qoff);
         const bool first_hop = FH == 1, last_hop = h + 1 >= v.hops;
         uint32_t *out_count = &cnt[h * n_views + vi];
         float4 *canvas = v.canvas;
@@ -997,6 +1010,195 @@ __global__ void __launch_bounds__(128, RF ? HT_WAVE_MINB : HT_PERSIST_MINB) rend
         }
     }
     flush_lane_stats(stats, st);
+}
+
+// ============================================================================ batch: coherence sort
+// The coherence sort of the single-view wavefronts, per view: the first `n_seg` hyperbolic
+// views of the launch order (the most expensive ones; at most BATCH_SORT_VIEWS) each get a
+// segment of SORT_BINS_VIEW bins of one histogram, and their queued paths a read order
+// within their own queue region. Position cells are kept per view and hop depth.
+constexpr uint32_t BATCH_SORT_VIEWS = 128;
+constexpr uint32_t SORT_BINS_VIEW = 96u * 512u;   // 48 blocks of the scan per view
+struct BatchSortBuf {
+    double *acc;        // per view and hop depth: 6 position sums
+    float *cut;         // per view and hop depth: 6 cell bounds
+    uint32_t *hist;     // BATCH_SORT_VIEWS x SORT_BINS_VIEW
+    uint32_t *bsum;     // scan block totals
+    uint32_t *cursor;   // as hist
+    uint32_t *seg_base; // per segment: cursor value at its first bin
+    uint16_t *key;      // per queue slot
+    uint32_t *perm;     // per queue slot: view-relative slot in sorted order
+};
+constexpr size_t batch_sort_head_bytes(uint32_t max_views, uint32_t hops) {   // acc, cut, hist
+    return (size_t)max_views * hops * SORT_DEPTH_WORDS * (sizeof(double) + sizeof(float)) +
+           sizeof(uint32_t) * (size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW;
+}
+constexpr size_t batch_sort_bytes(uint32_t max_views, uint32_t hops, uint64_t slots) {
+    return batch_sort_head_bytes(max_views, hops) +
+           sizeof(uint32_t) * ((size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW / 1024 + (size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW +
+                               BATCH_SORT_VIEWS) +
+           ((sizeof(uint16_t) * slots + 15) & ~(size_t)15) + sizeof(uint32_t) * slots;
+}
+static BatchSortBuf batch_sort_at(void *base, uint32_t max_views, uint32_t hops, uint64_t slots) {
+    BatchSortBuf b;
+    b.acc = reinterpret_cast<double *>(base);
+    b.cut = reinterpret_cast<float *>(b.acc + (size_t)max_views * hops * SORT_DEPTH_WORDS);
+    b.hist = reinterpret_cast<uint32_t *>(b.cut + (size_t)max_views * hops * SORT_DEPTH_WORDS);
+    b.bsum = b.hist + (size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW;
+    b.cursor = b.bsum + (size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW / 1024;
+    b.seg_base = b.cursor + (size_t)BATCH_SORT_VIEWS * SORT_BINS_VIEW;
+    b.key = reinterpret_cast<uint16_t *>(b.seg_base + BATCH_SORT_VIEWS);
+    b.perm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(b.key) + ((sizeof(uint16_t) * slots + 15) & ~(size_t)15));
+    return b;
+}
+
+// The views' path counts at queue depth h, as an exclusive prefix over the first n_seg
+// entries of `order` (s_pref: n_seg + 1 words), and the segment of the path numbered g.
+__device__ __forceinline__ void bsort_prefix(const BatchView *views, const uint32_t *order, uint32_t n_seg,
+                                             uint32_t n_views, uint32_t pass, uint32_t h, const uint32_t *cnt,
+                                             uint32_t *s_pref) {
+    for (uint32_t i = threadIdx.x; i < n_seg; i += blockDim.x) {
+        const uint32_t vi = order[i];
+        s_pref[i + 1] = batch_wave_count(views[vi], vi, pass, h, cnt, n_views);
+    }
+    if (threadIdx.x == 0) s_pref[0] = 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        uint32_t carry = 0;
+        for (uint32_t b0 = 0; b0 < n_seg; b0 += 32) {
+            const uint32_t i = b0 + lane;
+            uint32_t x = i < n_seg ? s_pref[i + 1] : 0;
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+                if (lane >= (uint32_t)off) x += y;
+            }
+            if (i < n_seg) s_pref[i + 1] = x + carry;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ uint32_t bsort_segment(const uint32_t *s_pref, uint32_t n_seg, uint32_t g) {
+    uint32_t lo = 0, hi = n_seg - 1;   // the last segment whose first path is <= g
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (s_pref[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Keys, histogram and position sums of the sorted views' paths at queue depth h. Block b
+// takes a contiguous range of the paths numbered over the views in order, so its position
+// sums (shared memory, n_seg x 6 floats) touch few views.
+__global__ void __launch_bounds__(SORT_THREADS) k_bsort_keys(const BatchView *__restrict__ views,
+                                                            const uint32_t *__restrict__ order, uint32_t n_seg,
+                                                            uint32_t n_views, uint32_t pass, uint32_t h,
+                                                            const uint32_t *cnt, uint32_t hops_max,
+                                                            const float4 *__restrict__ qp, const float4 *__restrict__ qv,
+                                                            const float *cut, double *acc, uint16_t *__restrict__ key,
+                                                            uint32_t *hist) {
+    extern __shared__ uint32_t s_pref[];                                  // n_seg + 1
+    float *s_acc = reinterpret_cast<float *>(s_pref + n_seg + 1);         // n_seg x 6
+    for (uint32_t i = threadIdx.x; i < 6 * n_seg; i += blockDim.x) s_acc[i] = 0.0f;
+    bsort_prefix(views, order, n_seg, n_views, pass, h, cnt, s_pref);
+    const uint32_t total = s_pref[n_seg];
+    const uint32_t per = ((total + gridDim.x - 1) / gridDim.x + 31) & ~31u;
+    const uint32_t g0 = blockIdx.x * per, g1 = min(total, g0 + per);
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t base = g0 + (threadIdx.x >> 5) * 32u; base < g1; base += SORT_THREADS) {
+        const uint32_t g = base + lane;
+        const bool valid = g < g1;
+        uint32_t bin = 0x80000000u + lane;   // lanes past the end group alone
+        uint32_t sg = 0;
+        float m[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (valid) {
+            sg = bsort_segment(s_pref, n_seg, g);
+            const uint32_t vi = order[sg];
+            const uint64_t slot = views[vi].qoff + (g - s_pref[sg]);
+            const float *c = cut + ((size_t)vi * hops_max + h) * SORT_DEPTH_WORDS;
+            const float4 q = qp[slot];
+            const float l = sort_logz(q.z);
+            m[0] = q.x; m[1] = q.x * q.x;
+            m[2] = q.y; m[3] = q.y * q.y;
+            m[4] = l;   m[5] = l * l;
+            const uint32_t cx = sort_axis_cell(q.x, c[0], c[3]);
+            const uint32_t cy = sort_axis_cell(q.y, c[1], c[4]);
+            const uint32_t cz = sort_axis_cell(l, c[2], c[5]);
+            const uint32_t k = sort_dir_cell(qv[slot]) * 512u + (spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2));
+            key[slot] = (uint16_t)k;
+            bin = sg * SORT_BINS_VIEW + k;
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, bin);
+        if (valid && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&hist[bin], (uint32_t)__popc(grp));
+        // position sums: one add per value when the warp's paths are one view's (lane 0 is
+        // always a path here), else one per lane
+        const uint32_t sg0 = __shfl_sync(0xffffffffu, sg, 0);
+        if (__all_sync(0xffffffffu, !valid || sg == sg0)) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                for (int o = 16; o; o >>= 1) m[q] += __shfl_xor_sync(0xffffffffu, m[q], o);
+                if (lane == 0) atomicAdd(&s_acc[6 * sg0 + q], m[q]);
+            }
+        } else if (valid) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) atomicAdd(&s_acc[6 * sg + q], m[q]);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 6 * n_seg; i += blockDim.x)
+        if (s_acc[i] != 0.0f)
+            atomicAdd(&acc[((size_t)order[i / 6] * hops_max + h) * SORT_DEPTH_WORDS + i % 6], (double)s_acc[i]);
+}
+
+// Sorted positions of the sorted views' paths at queue depth h: perm[qoff + position] =
+// view-relative slot. Block 0 first turns each view's position sums into its cells for the
+// next pass (the keys of this pass are already made) and clears the sums.
+__global__ void __launch_bounds__(SORT_THREADS) k_bsort_scatter(const BatchView *__restrict__ views,
+                                                               const uint32_t *__restrict__ order, uint32_t n_seg,
+                                                               uint32_t n_views, uint32_t pass, uint32_t h,
+                                                               const uint32_t *cnt, uint32_t hops_max,
+                                                               const uint16_t *__restrict__ key, uint32_t *cursor,
+                                                               const uint32_t *seg_base, double *acc, float *cut,
+                                                               uint32_t *__restrict__ perm) {
+    extern __shared__ uint32_t s_pref[];   // n_seg + 1
+    bsort_prefix(views, order, n_seg, n_views, pass, h, cnt, s_pref);
+    if (blockIdx.x == 0)
+        for (uint32_t i = threadIdx.x; i < 3 * n_seg; i += blockDim.x) {
+            const uint32_t sg = i / 3, ax = i % 3;
+            const size_t d = ((size_t)order[sg] * hops_max + h) * SORT_DEPTH_WORDS;
+            const uint32_t n = s_pref[sg + 1] - s_pref[sg];
+            if (n) {
+                const double mean = acc[d + 2 * ax] / (double)n;
+                const double sd = sqrt(fmax(acc[d + 2 * ax + 1] / (double)n - mean * mean, 0.0));
+                cut[d + ax] = (float)(mean - 2.0 * sd);
+                cut[d + 3 + ax] = sd > 0.0 ? (float)(2.0 / sd) : 0.0f;
+            }
+            acc[d + 2 * ax] = 0.0;
+            acc[d + 2 * ax + 1] = 0.0;
+        }
+    const uint32_t total = s_pref[n_seg];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (SORT_THREADS / 32);
+    for (uint32_t base = (blockIdx.x * (SORT_THREADS / 32) + (threadIdx.x >> 5)) * 32u; base < total; base += warps * 32u) {
+        const uint32_t g = base + lane;
+        const bool valid = g < total;
+        uint32_t bin = 0x80000000u + lane, sg = 0, j = 0;
+        uint64_t qoff = 0;
+        if (valid) {
+            sg = bsort_segment(s_pref, n_seg, g);
+            j = g - s_pref[sg];
+            qoff = views[order[sg]].qoff;
+            bin = sg * SORT_BINS_VIEW + key[qoff + j];
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, bin);
+        const int leader = __ffs(grp) - 1;
+        uint32_t at = 0;
+        if (valid && lane == (uint32_t)leader) at = atomicAdd(&cursor[bin], (uint32_t)__popc(grp)) - seg_base[sg];
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (valid) perm[qoff + at + __popc(grp & ((1u << lane) - 1u))] = j;
+    }
 }
 
 // ============================================================================ double_support
@@ -1502,7 +1704,8 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
                 float *cut = sb.cut + (size_t)h * SORT_DEPTH_WORDS;
                 k_sort_keys<<<sort_blocks, SORT_THREADS, 0, st>>>(in.p, in.v, in_count, cut, acc, sb.key, sb.hist);
                 k_sort_scan_blocks<<<SORT_SCAN_BLOCKS, SORT_THREADS, 0, st>>>(sb.hist, sb.bsum);
-                k_sort_scan<<<SORT_SCAN_BLOCKS, SORT_THREADS, 0, st>>>(sb.hist, sb.bsum, sb.cursor, acc, cut, in_count);
+                k_sort_scan<<<SORT_SCAN_BLOCKS, SORT_THREADS, 0, st>>>(sb.hist, sb.bsum, sb.cursor, SORT_BINS, nullptr,
+                                                                      acc, cut, in_count);
                 k_sort_scatter<<<sort_blocks, SORT_THREADS, 0, st>>>(sb.key, in_count, sb.cursor, sb.perm);
                 in.o = sb.perm;
             }
@@ -1674,6 +1877,9 @@ struct htc_batch {
     uint64_t wave_slots;     // slots per queue
     uint32_t *d_wcnt;
     size_t wcnt_words;
+    void *sort_buf;          // coherence sort of the hyperbolic views (BatchSortBuf)
+    uint64_t sort_slots;     // = wave_slots when allocated
+    uint32_t sort_hops;
 };
 
 static void batch_free(htc_batch *b) {
@@ -1689,6 +1895,7 @@ static void batch_free(htc_batch *b) {
     if (b->d_order) cudaFree(b->d_order);
     if (b->wave_buf) cudaFree(b->wave_buf);
     if (b->d_wcnt) cudaFree(b->d_wcnt);
+    if (b->sort_buf) cudaFree(b->sort_buf);
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_views);
@@ -1734,6 +1941,11 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
     const size_t words = (size_t)(b->n_views + 3) * b->hops_max;
     uint32_t *grab = b->d_wcnt + (size_t)b->n_views * b->hops_max;   // 3 words per hop depth
     const uint32_t *order_hy = b->d_order + b->n_order, *order_eu = order_hy + b->n_hy;
+    // coherence sort of the first n_seg hyperbolic views in launch order (the expensive ones)
+    const uint32_t n_seg = HT_BATCH_SORT && HT_BATCH_SPLIT && b->sort_buf ? std::min(b->n_hy, BATCH_SORT_VIEWS) : 0u;
+    const BatchSortBuf sb = n_seg ? batch_sort_at(b->sort_buf, b->max_views, b->sort_hops, b->sort_slots) : BatchSortBuf{};
+    const unsigned sort_blocks = (unsigned)b->num_sms * 8u;
+    const size_t keys_smem = sizeof(uint32_t) * (n_seg + 1) + sizeof(float) * 6 * n_seg;
     for (uint32_t pass = 0; pass < b->passes_max; ++pass) {
         HTC_CUDA(cudaMemsetAsync(b->d_wcnt, 0, sizeof(uint32_t) * words, st));
         for (uint32_t h = 0; h < b->hops_max; ++h) {
@@ -1741,19 +1953,33 @@ static int batch_launch_wave(htc_batch *b, uint64_t *stats, cudaStream_t st) {
             if (!HT_BATCH_SPLIT) {
                 (h == 0 ? render_batch_wave<0, 1> : render_batch_wave<0, 2>)<<<blocks_any, 128, smem, st>>>(b->d_views, b->d_order, b->n_order, b->n_views, pass,
                                                                    h, b->tile_pixels, b->smem_objects, in, out,
-                                                                   b->d_wcnt, grab + 3 * h, stats, b->d_err);
+                                                                   b->d_wcnt, grab + 3 * h, stats, b->d_err, 0u);
                 continue;
+            }
+            WaveQueue in_hy = in;
+            if (n_seg && h > 0) {
+                k_bsort_keys<<<sort_blocks, SORT_THREADS, keys_smem, st>>>(b->d_views, order_hy, n_seg, b->n_views, pass, h,
+                                                                          b->d_wcnt, b->hops_max, in.p, in.v, sb.cut,
+                                                                          sb.acc, sb.key, sb.hist);
+                k_sort_scan_blocks<<<n_seg * (SORT_BINS_VIEW / 1024), SORT_THREADS, 0, st>>>(sb.hist, sb.bsum);
+                k_sort_scan<<<n_seg * (SORT_BINS_VIEW / 1024), SORT_THREADS, 0, st>>>(sb.hist, sb.bsum, sb.cursor,
+                                                                                     SORT_BINS_VIEW, sb.seg_base, nullptr,
+                                                                                     nullptr, nullptr);
+                k_bsort_scatter<<<sort_blocks, SORT_THREADS, sizeof(uint32_t) * (n_seg + 1), st>>>(
+                    b->d_views, order_hy, n_seg, b->n_views, pass, h, b->d_wcnt, b->hops_max, sb.key, sb.cursor,
+                    sb.seg_base, sb.acc, sb.cut, sb.perm);
+                in_hy.o = sb.perm;
             }
             if (b->n_hy)
                 (h == 0 ? render_batch_wave<RECIPE_HY, 1> : render_batch_wave<RECIPE_HY, 2>)<<<blocks_hy, 128, smem, st>>>(b->d_views, order_hy, b->n_hy, b->n_views,
-                                                                           pass, h, b->tile_pixels, b->smem_objects, in,
+                                                                           pass, h, b->tile_pixels, b->smem_objects, in_hy,
                                                                            out, b->d_wcnt, grab + 3 * h + 1, stats,
-                                                                           b->d_err);
+                                                                           b->d_err, n_seg);
             if (b->n_eu)
                 (h == 0 ? render_batch_wave<RECIPE_EU, 1> : render_batch_wave<RECIPE_EU, 2>)<<<blocks_eu, 128, smem, st>>>(b->d_views, order_eu, b->n_eu, b->n_views,
                                                                            pass, h, b->tile_pixels, b->smem_objects, in,
                                                                            out, b->d_wcnt, grab + 3 * h + 2, stats,
-                                                                           b->d_err);
+                                                                           b->d_err, 0u);
         }
         HTC_CUDA(cudaGetLastError());
     }
@@ -1801,8 +2027,10 @@ void htc_batch_destroy(htc_batch *b) { batch_free(b); }
 
 // Grows the wavefront queues (slots per queue) and counters (words) when a view set needs
 // more; launches already enqueued on `st` may still use the old ones, so they finish first.
-static int batch_grow(htc_batch *b, uint64_t slots, size_t words, cudaStream_t st) {
-    if (slots <= b->wave_slots && words <= b->wcnt_words) return HTC_OK;
+static int batch_grow(htc_batch *b, uint64_t slots, size_t words, uint32_t hops, cudaStream_t st) {
+    if (slots <= b->wave_slots && words <= b->wcnt_words && (!HT_BATCH_SORT || (b->sort_slots >= b->wave_slots &&
+                                                                              hops <= b->sort_hops)))
+        return HTC_OK;
     HTC_CUDA(cudaStreamSynchronize(st));
     if (slots > b->wave_slots) {
         if (b->wave_buf) HTC_CUDA(cudaFree(b->wave_buf));
@@ -1819,6 +2047,17 @@ static int batch_grow(htc_batch *b, uint64_t slots, size_t words, cudaStream_t s
         HTC_CUDA(cudaMalloc(&b->d_wcnt, sizeof(uint32_t) * words));
         b->wcnt_words = words;
     }
+    if (HT_BATCH_SORT && (b->sort_slots < b->wave_slots || hops > b->sort_hops)) {
+        if (b->sort_buf) HTC_CUDA(cudaFree(b->sort_buf));
+        b->sort_buf = nullptr;
+        b->sort_slots = 0;
+        const uint32_t sh = std::max(hops, b->sort_hops);
+        HTC_CUDA(cudaMalloc(&b->sort_buf, batch_sort_bytes(b->max_views, sh, b->wave_slots)));
+        // sums, cells and histogram start cleared; the sort launches clear sums and histogram after each use
+        HTC_CUDA(cudaMemset(b->sort_buf, 0, batch_sort_head_bytes(b->max_views, sh)));
+        b->sort_slots = b->wave_slots;
+        b->sort_hops = sh;
+    }
     return HTC_OK;
 }
 
@@ -1828,7 +2067,7 @@ int htc_batch_reserve(htc_batch *b, uint64_t pixels, uint32_t max_hops, void *st
     if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
     if (max_hops == 0) return fail(HTC_ERR_INVALID, "max_hops must be positive");
     // each view's region is rounded up to 64 slots
-    return batch_grow(b, pixels + 64ull * b->max_views, (size_t)(b->max_views + 3) * max_hops,
+    return batch_grow(b, pixels + 64ull * b->max_views, (size_t)(b->max_views + 3) * max_hops, max_hops,
                       reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -1890,7 +2129,7 @@ int htc_batch_set_views(htc_batch *b, const htc_view *views, uint32_t n_views, u
     b->tile_pixels = tile_pixels;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     {
-        int rc = batch_grow(b, slots, (size_t)(n_views + 3) * hops_max, st);
+        int rc = batch_grow(b, slots, (size_t)(n_views + 3) * hops_max, hops_max, st);
         if (rc) return rc;
     }
     b->n_views = n_views;
