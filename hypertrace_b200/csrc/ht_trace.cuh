@@ -223,14 +223,13 @@ static __device__ __noinline__ HyPath camera_hy(const StagedScene &s, float px, 
 #ifndef HT_EST_OBJECTS
 #define HT_EST_OBJECTS 32u
 #endif
-struct PairRay { float2 r2, x, y, K, nK; };   // the bound ray's constants, each in both halves
+struct PairRay { float2 r2, x, y, K; };   // the bound ray's constants, each in both halves
 HT_D PairRay pair_ray(const BoundRay &r) {
     PairRay p;
     p.r2 = make_float2(r.r2, r.r2);
     p.x = make_float2(r.x, r.x);
     p.y = make_float2(r.y, r.y);
     p.K = make_float2(r.K, r.K);
-    p.nK = make_float2(-r.K, -r.K);
     return p;
 }
 HT_D uint32_t survivors2(float4 a, float4 b, float2 mag, const PairRay &r, const PointCut &k) {
@@ -238,8 +237,9 @@ HT_D uint32_t survivors2(float4 a, float4 b, float2 mag, const PairRay &r, const
     float2 F = __ffma2_rn(make_float2(b.x, b.y), r.y, make_float2(b.z, b.w));
     F = __ffma2_rn(make_float2(a.z, a.w), r.x, F);
     F = __ffma2_rn(make_float2(a.x, a.y), r.r2, F);
-    const float2 up = __fadd2_rn(F, __fmul2_rn(mag, r.K));     // F + eF
-    const float2 dn = __fadd2_rn(F, __fmul2_rn(mag, r.nK));    // F - eF (m (-K) = -(m K) exactly)
+    const float2 e = __fmul2_rn(mag, r.K);                      // eF, once for both sides
+    const float2 up = __fadd2_rn(F, e);                          // F + eF
+    const float2 dn = __fadd2_rn(F, make_float2(-e.x, -e.y));   // F - eF
     const bool c0 = up.x < k.lo.x || dn.x > k.hi.x;
     const bool c1 = up.y < k.lo.y || dn.y > k.hi.y;
     return (c0 ? 0u : 1u) | (c1 ? 0u : 2u);
@@ -264,9 +264,69 @@ HT_D float upper_estimate(const StagedScene &s, const BoundRay &r, uint32_t prev
     return best < __int_as_float(0x7f800000) ? dist_from_e2(best) : best;
 }
 
-template <bool OOL>
+// Warp pre-cull (wavefront kernels, full warps whose lanes can all cull): each lane tests
+// one slot of a 32-slot chunk against the whole warp at once — F over the box of the lanes'
+// (|p|^2, x, y), the largest error allowance and the loosest thresholds of the warp — and a
+// slot the warp test culls is culled by every lane's own point test, so the lanes run that
+// test only on the pairs the warp keeps and reach the same candidate masks bit for bit. The
+// warp test adds a slack of 2^-16 of the magnitudes involved, far above the rounding of
+// either evaluation (a few units of 2^-24 each), so float rounding cannot break that
+// implication. After the coherence sort a warp's rays start in one cell, the box is small,
+// and most slots go in one test per warp instead of one per lane.
+struct WarpBox { float r2lo, r2hi, xlo, xhi, ylo, yhi, K; };
+HT_D uint32_t ord_bits(float f) {   // order-preserving map of floats (no NaN) to unsigned
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+HT_D float ord_float(uint32_t o) { return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o); }
+HT_D float warp_min(float f) { return ord_float(__reduce_min_sync(0xffffffffu, ord_bits(f))); }
+HT_D float warp_max(float f) { return ord_float(__reduce_max_sync(0xffffffffu, ord_bits(f))); }
+HT_D WarpBox warp_box(const BoundRay &r) {
+    WarpBox b;
+    b.r2lo = warp_min(r.r2); b.r2hi = warp_max(r.r2);
+    b.xlo = warp_min(r.x);   b.xhi = warp_max(r.x);
+    b.ylo = warp_min(r.y);   b.yhi = warp_max(r.y);
+    b.K = warp_max(r.K);
+    return b;
+}
+// interval of a * u over u in [lo, hi], and a bound of |a u| there
+HT_D void box_term(float a, float lo, float hi, float &flo, float &fhi, float &mag) {
+    const float p = a * lo, q = a * hi;
+    flo += fminf(p, q);
+    fhi += fmaxf(p, q);
+    mag += fmaxf(fabsf(p), fabsf(q));
+}
+// Slots of chunk [c0, c0 + cn) that some lane of the warp may keep (every lane calls this).
+HT_D uint32_t warp_survivors(const StagedScene &s, uint32_t c0, uint32_t valid, const WarpBox &b,
+                             const PointCut &kp, const PointCut &kh) {
+    const uint32_t lane = threadIdx.x & 31;
+    const float hp = warp_max(kp.hi.x);   // planes: lo = -hi
+    const float lh = warp_min(kh.lo.x), hh = warp_max(kh.hi.x);
+    bool keep = false;
+    if (valid >> lane & 1u) {
+        const uint32_t q = c0 + lane;
+        const float4 rec = s.bound[q];
+        const float e = s.mag[q] * b.K;
+        float flo = rec.w, fhi = rec.w, mag = fabsf(rec.w);
+        box_term(rec.x, b.r2lo, b.r2hi, flo, fhi, mag);
+        box_term(rec.y, b.xlo, b.xhi, flo, fhi, mag);
+        box_term(rec.z, b.ylo, b.yhi, flo, fhi, mag);
+        const float slack = 0x1p-16f * (mag + e);
+        float lo = lh, hi = hh;
+        if (s.shape[q] == 0) {
+            lo = -hp;
+            hi = hp;
+        }
+        keep = !((fhi + e) + slack < lo || (flo - e) - slack > hi);   // NaN: kept
+    }
+    return __ballot_sync(0xffffffffu, keep);
+}
+
+// WARP: the warp pre-cull is compiled in; `full_warp` (all 32 lanes of the warp are in this
+// call together, uniform across the warp) turns it on.
+template <bool OOL, bool WARP = false>
 HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &prev_hash,
-                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact) {
+                 Col &intensity, Col &emission, bool &hit, uint32_t &n_exact, bool full_warp = false) {
     // Nearest hit with ties to the lowest scene index (object/vector.inl:37-50): candidates
     // are compared on (distance, index), so the order of the slots does not matter; x =
     // cosh(distance) is compared first and the logarithm taken only when x can win; objects
@@ -284,6 +344,15 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
         if (u < __int_as_float(0x7f800000)) cull = cull_from_dist(u);
     }
     PointCut kp = point_cut(0, br.t, cull), kh = point_cut(1, br.t, cull);
+    bool warp_pre = false;
+    WarpBox wb;
+    if constexpr (WARP) {
+        if (full_warp) {
+            __syncwarp();
+            warp_pre = __all_sync(0xffffffffu, can_cull);
+            if (warp_pre) wb = warp_box(br);
+        }
+    }
     for (uint32_t c0 = 0; c0 < s.ns; c0 += 32) {
         const uint32_t cn = min(32u, s.ns - c0);
         uint32_t valid = cn == 32 ? 0xFFFFFFFFu : (1u << cn) - 1u;
@@ -291,12 +360,27 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
         uint32_t mask = valid;
         if (can_cull) {
             mask = 0;
-            // kept rolled: the kernel is bound by instruction fetch as much as by issue
+            if (WARP && warp_pre) {   // uniform: every lane can cull
+                __syncwarp();
+                const uint32_t keep = warp_survivors(s, c0, valid, wb, kp, kh);
+                // this lane's point test on the pairs with a slot the warp keeps
+                uint32_t pm = (keep | (keep >> 1)) & 0x55555555u;
+                while (pm) {
+                    const uint32_t j = __ffs(pm) - 1;
+                    pm &= pm - 1;
+                    const uint32_t pq = (c0 + j) >> 1;
+                    const PointCut &k = c0 + j >= s.n_planes ? kh : kp;
+                    mask |= survivors2(s.pa[pq], s.pb[pq], s.pmag[pq], pr, k) << j;
+                }
+                mask &= keep;
+            } else {
+                // kept rolled: the kernel is bound by instruction fetch as much as by issue
 #pragma unroll 1
-            for (uint32_t j = 0; j < cn; j += 2) {   // warp-uniform: broadcast loads, two slots at once
-                const uint32_t pq = (c0 + j) >> 1;
-                const PointCut &k = c0 + j >= s.n_planes ? kh : kp;
-                mask |= survivors2(s.pa[pq], s.pb[pq], s.pmag[pq], pr, k) << j;
+                for (uint32_t j = 0; j < cn; j += 2) {   // warp-uniform: broadcast loads, two slots at once
+                    const uint32_t pq = (c0 + j) >> 1;
+                    const PointCut &k = c0 + j >= s.n_planes ? kh : kp;
+                    mask |= survivors2(s.pa[pq], s.pb[pq], s.pmag[pq], pr, k) << j;
+                }
             }
             mask &= valid;
             // per lane: the ray-aware bound on the survivors only

@@ -290,11 +290,14 @@ __device__ __forceinline__ typename PathOf<R>::T camera(const StagedScene &s, fl
     if constexpr (R == RECIPE_HY) return camera_hy(s, px, py, size, rng, flags);
     else return camera_eu(s, px, py, size, rng, flags);
 }
-template <int R, bool OOL = true>
+// WARP / full_warp: the hyperbolic scan's warp pre-cull (hop_hy), for callers whose warps
+// enter together.
+template <int R, bool OOL = true, bool WARP = false>
 __device__ __forceinline__ bool hop(const StagedScene &s, typename PathOf<R>::T &ray, uint32_t &rng,
                                     uint32_t &prev_hash, Col &intensity, Col &emission, bool &hit,
-                                    uint32_t &n_exact) {
-    if constexpr (R == RECIPE_HY) return hop_hy<OOL>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
+                                    uint32_t &n_exact, bool full_warp = false) {
+    if constexpr (R == RECIPE_HY)
+        return hop_hy<OOL, WARP>(s, ray, rng, prev_hash, intensity, emission, hit, n_exact, full_warp);
     else return hop_eu(s, ray, rng, prev_hash, intensity, emission, hit, n_exact);
 }
 
@@ -575,6 +578,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
     Col intensity = {1.0f, 1.0f, 1.0f};
     Col emission = {0.0f, 0.0f, 0.0f};
     const bool first = FH == 1 || (FH == 0 && first_hop);
+    const bool full_warp = __ballot_sync(0xffffffffu, i < n) == 0xffffffffu;   // every lane has a path
     if (i < n) {
         if (first) {
             pixel = i;
@@ -595,7 +599,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
         bool hit;
         st.hops += 1;
         st.tests += s.n;
-        const bool go = hop<R, OOL>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact);
+        const bool go = hop<R, OOL, true>(s, ray, rng, prev_hash, intensity, emission, hit, st.exact, full_warp);
         st.hits += hit ? 1 : 0;
         cont = go && !last_hop;
         if (!cont) {
