@@ -360,12 +360,16 @@ HT_D bool hop_hy(const StagedScene &s, HyPath &ray, uint32_t &rng, uint32_t &pre
         uint32_t mask = valid;
         if (can_cull) {
             mask = 0;
-            if (WARP && warp_pre) {   // uniform: every lane can cull
-                __syncwarp();
-                const uint32_t keep = warp_survivors(s, c0, valid, wb, kp, kh);
-                // this lane's point test on the pairs with a slot the warp keeps
+            if constexpr (WARP) {
+                // one copy of the pair loop for both cases (instruction fetch): over the pairs
+                // with a slot the warp keeps, or over every valid pair without the warp test
+                uint32_t keep = valid;
+                if (warp_pre) {   // uniform: every lane can cull
+                    __syncwarp();
+                    keep = warp_survivors(s, c0, valid, wb, kp, kh);
+                }
                 uint32_t pm = (keep | (keep >> 1)) & 0x55555555u;
-                while (pm) {
+                while (pm) {   // this lane's point test
                     const uint32_t j = __ffs(pm) - 1;
                     pm &= pm - 1;
                     const uint32_t pq = (c0 + j) >> 1;
