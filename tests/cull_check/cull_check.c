@@ -28,7 +28,7 @@ static float adv(float x, int dir) { return ADV ? x * (1.0f + (float)dir * ADV_E
 #define CULL_ABS 1e-2f
 #define BOUND_EPS 1e-5f
 #define HORO_M 1e-3f
-#define EST_OBJECTS 32u
+#define EST_OBJECTS 24u
 #define LN2F 0.693147180559945f
 #define LOG2EF 1.442695040888963f
 

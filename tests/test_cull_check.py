@@ -6,7 +6,7 @@ of sampled paths, both the full scan of the reference and the culled scan of the
 must pick the same object at the same distance. In adversarial mode each value the kernel
 takes from a PTX approximation is pushed 2^-21 relative (beyond that instruction's error) the
 way that culls more. CPU only: the exact-test rate it counts on the 1080p frame is also the
-one the GPU's statistics counter reports there (3.02 per hop with the slots planes first).
+one the GPU's statistics counter reports there (3.19 per hop with the slots planes first and the estimate over 12 + 12 objects).
 """
 import os
 import subprocess
@@ -42,7 +42,7 @@ def test_headline_frame(checker, tmp_path, adversarial):
     wl = S.config2()
     hops, exact, wrong = _run(checker, tmp_path, wl.scene, wl.width, wl.height, 6000, wl.global_seed, adversarial)
     assert hops > 20000 and wrong == 0
-    assert 2.8 < exact < 3.2   # 200 objects per hop without culling
+    assert 3.0 < exact < 3.4   # 200 objects per hop without culling
 
 
 @pytest.mark.parametrize("seed", [11, 12, 13])
