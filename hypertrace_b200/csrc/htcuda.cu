@@ -43,15 +43,21 @@ thread_local std::string g_last_error;
 // Measured on the current code at 1080p / 200 objects (Msamples/s): 7 -> 6 -> 5 blocks (72 ->
 // 80 -> 96 registers) took the wavefront kernel 368.6 -> 373.2 -> 377.4 and the batched mix
 // (spp / 16) 994 -> 1012 -> 1019; the one-pass kernel 288.6 -> 296.5 -> 295.6. The earlier
-// scan had measured 7 best (239.5 against 232 for 6).
+// scan had measured 7 best (239.5 against 232 for 6). With the coherence sort and the warp
+// pre-cull, 6 -> 5 -> 4 blocks gave the single-view wavefront kernel 489.5 -> 493.0 -> 508.1
+// and the batched kernels (mix at spp / 16) 1170.8 -> 1210.2 -> 1172.2, so the two now have
+// caps of their own.
 #ifndef HT_PERSIST_MINB
 #define HT_PERSIST_MINB 6
 #endif
 #ifndef HT_PLAIN_MINB
 #define HT_PLAIN_MINB 6
 #endif
-#ifndef HT_WAVE_MINB
-#define HT_WAVE_MINB 5
+#ifndef HT_WAVE_MINB    // render_wave
+#define HT_WAVE_MINB 4
+#endif
+#ifndef HT_BATCH_MINB   // render_batch_wave (one recipe per kernel)
+#define HT_BATCH_MINB 5
 #endif
 // htc_render_passes: 2 = wavefronts (one launch per hop depth), 1 = the persistent kernel,
 // 0 = one launch of the one-pass kernel per pass. All three give the same bits. Measured at
@@ -60,10 +66,10 @@ thread_local std::string g_last_error;
 #ifndef HT_PASSES_MODE
 #define HT_PASSES_MODE 2
 #endif
-// Batched wavefronts: 1 = one launch per recipe for each (pass, hop depth), 0 = one launch for both.
 #ifndef HT_BATCH_SORT   // coherence sort of the batch's hyperbolic views (with HT_BATCH_SPLIT)
 #define HT_BATCH_SORT 1
 #endif
+// Batched wavefronts: 1 = one launch per recipe for each (pass, hop depth), 0 = one launch for both.
 #ifndef HT_BATCH_SPLIT
 #define HT_BATCH_SPLIT 1
 #endif
@@ -894,7 +900,7 @@ __device__ __forceinline__ uint32_t batch_wave_count(const BatchView &v, uint32_
 // RF = 0 serves views of either recipe (a runtime branch per tile); RF = RECIPE_HY or
 // RECIPE_EU compiles one recipe only (its views alone in `order`), with fewer registers.
 template <int RF, int FH>
-__global__ void __launch_bounds__(128, RF ? HT_WAVE_MINB : HT_PERSIST_MINB) render_batch_wave(
+__global__ void __launch_bounds__(128, RF ? HT_BATCH_MINB : HT_PERSIST_MINB) render_batch_wave(
     const BatchView *__restrict__ views, const uint32_t *__restrict__ order, uint32_t n_order, uint32_t n_views,
     uint32_t pass, uint32_t h, uint32_t tile_slots, uint32_t smem_objects, WaveQueue in, WaveQueue out,
     uint32_t *cnt, uint32_t *grab, uint64_t *stats, uint32_t *err, uint32_t n_sorted) {
