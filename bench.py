@@ -52,9 +52,9 @@ UNIT = "Msamples/s"
 # FMUL, twice that for their packed forms (FFMA2 / FADD2 / FMUL2); instructions are warp
 # instructions issued; DRAM bytes are read + written. Frozen from that capture (the summary with
 # the command is profiles/render_wave_hy1080p_200obj.md): re-capture after a kernel change.
-FP32_OPS_PER_HOP = 4495.1       # 44.10e9 per pass over 9.81e6 path-hops
-WARP_INSTR_PER_HOP = 307.99     # 3.022e9 per pass
-DRAM_BYTES_PER_HOP = 154.46     # 1.515e9 per pass
+FP32_OPS_PER_HOP = 4243.3       # 41.63e9 per pass over 9.81e6 path-hops
+WARP_INSTR_PER_HOP = 284.84     # 2.794e9 per pass
+DRAM_BYTES_PER_HOP = 147.77     # 1.450e9 per pass
 # The reference's own FP32 count per hop for comparison: every object's detect maps the ray in
 # and out (two ray maps of 256 operations, object/mapped.inl:32,34, plus the shape test), i.e.
 # 527 per object and hop. Distance culling skips 98 % of those tests, so this count can exceed

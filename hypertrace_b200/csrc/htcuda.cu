@@ -53,8 +53,11 @@ thread_local std::string g_last_error;
 #ifndef HT_PLAIN_MINB
 #define HT_PLAIN_MINB 6
 #endif
-#ifndef HT_WAVE_MINB    // render_wave
+#ifndef HT_WAVE_MINB    // render_wave, hop depths after the first
 #define HT_WAVE_MINB 4
+#endif
+#ifndef HT_WAVE0_MINB   // render_wave, hop depth 0 (camera rays: 0.764 ms per launch at 5, 0.792 at 4)
+#define HT_WAVE0_MINB 5
 #endif
 #ifndef HT_BATCH_MINB   // render_batch_wave (one recipe per kernel)
 #define HT_BATCH_MINB 5
@@ -635,7 +638,7 @@ __device__ __forceinline__ void wave_chunk(const StagedScene &s, uint32_t base, 
 // ctr[0]: slots taken by warps of this launch; ctr[1]: paths appended to `out`.
 // in_count: paths in `in` (NULL for hop 0, which covers the W*H pixels).
 template <int R, int FH>
-__global__ void __launch_bounds__(128, HT_WAVE_MINB) render_wave(
+__global__ void __launch_bounds__(128, FH == 1 ? HT_WAVE0_MINB : HT_WAVE_MINB) render_wave(
     const uint8_t *__restrict__ scene, size_t scene_size, uint32_t max_objects, int address_width,
     uint32_t W, uint32_t H, uint32_t hops, uint32_t hop_index, uint32_t flags, float4 *__restrict__ canvas,
     uint32_t *__restrict__ seeds, uint64_t *stats, uint32_t *err, WaveQueue in, const uint32_t *in_count,
@@ -1693,11 +1696,15 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
                        uint32_t max_objects, size_t smem, float4 *cv, uint32_t *seeds, uint32_t passes,
                        uint64_t *stats, cudaStream_t st) {
     int per_sm = 0;
+    // a grid per kernel: the hop-0 and later-hop kernels have register caps of their own
+    int per_sm0 = 0;
     HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_wave<R, 2>, 128, smem));
+    HTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, render_wave<R, 1>, 128, smem));
     if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)per_sm * (uint64_t)p->num_sms;
+    if (per_sm0 < 1) per_sm0 = 1;
     const uint64_t needed = ((uint64_t)W * H + 127) / 128;
-    if (blocks > needed) blocks = needed;
+    const uint64_t blocks = std::min<uint64_t>((uint64_t)per_sm * (uint64_t)p->num_sms, needed);
+    const uint64_t blocks0 = std::min<uint64_t>((uint64_t)per_sm0 * (uint64_t)p->num_sms, needed);
     const WaveQueue q[2] = {wave_queue(p, 0), wave_queue(p, 1)};
     const WaveQueue none = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     const bool sorted = R == RECIPE_HY && p->sort_buf != nullptr && !(p->flags & HTC_FLAG_NO_SORT);
@@ -1719,7 +1726,7 @@ static int launch_wave(htc_program *p, uint32_t W, uint32_t H, const uint8_t *sc
                 k_sort_scatter<<<sort_blocks, SORT_THREADS, 0, st>>>(sb.key, in_count, sb.cursor, sb.perm);
                 in.o = sb.perm;
             }
-            (h == 0 ? render_wave<R, 1> : render_wave<R, 2>)<<<(unsigned)blocks, 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
+            (h == 0 ? render_wave<R, 1> : render_wave<R, 2>)<<<(unsigned)(h == 0 ? blocks0 : blocks), 128, smem, st>>>(sc, scene_size, max_objects, p->address_width, W, H,
                                                                p->hops, h, p->flags, cv, seeds, stats, p->d_err, in,
                                                                in_count, q[h & 1], p->d_wave_ctr + 2 * h);
         }
