@@ -185,6 +185,7 @@ static uint32_t fmix32(uint32_t h) {
     h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16; return h;
 }
 
+#ifndef CULL_CHECK_NO_MAIN
 int main(int argc, char **argv) {
     if (argc < 8) { fprintf(stderr, "usage\n"); return 2; }
     FILE *f = fopen(argv[1], "rb");
@@ -297,3 +298,4 @@ int main(int argc, char **argv) {
     scene_free(&sc);
     return 0;
 }
+#endif  /* CULL_CHECK_NO_MAIN */

@@ -52,3 +52,39 @@ def test_random_scenes(checker, tmp_path, seed):
     hops, exact, wrong = _run(checker, tmp_path, sc, 640, 480, 3000, seed, True)
     assert hops > 5000 and wrong == 0
     assert exact < 20
+
+
+WARP_SRC = os.path.join(HERE, "cull_check", "warp_check.c")
+
+
+@pytest.fixture(scope="module")
+def warp_checker(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("warp") / "warp_check")
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-o", exe, WARP_SRC, "-lm", "-lpthread"],
+                   check=True)
+    return exe
+
+
+@pytest.mark.parametrize("seed", [None, 21, 22])
+def test_warp_precull_implies_every_lane_culls(warp_checker, tmp_path, seed):
+    """The wavefront scan's warp pre-cull (ht_trace.cuh warp_survivors) may drop a slot for a
+    whole warp only if every lane's own point test drops it too, in float arithmetic: both
+    tests restated op for op (tests/cull_check/warp_check.c), on warps of the coherence sort's
+    order and on tight warps (starts a few ulps apart), where the 2^-16 slack is all that
+    separates the two tests. A slack 2^-20 on the wrong side gives violations there."""
+    if seed is None:
+        wl = S.config2()
+        scene, W, H, gs = wl.scene, wl.width, wl.height, wl.global_seed
+    else:
+        rng = np.random.default_rng(seed)
+        scene = S.hyperbolic_scene(40, 90, 6.0, 8, 800 + seed, camera=S.random_moebius(rng, 1.0))
+        W, H, gs = 1280, 720, seed
+    path = tmp_path / "scene.bin"
+    path.write_bytes(scene.to_bytes())
+    out = subprocess.run([warp_checker, str(path), str(W), str(H), str(scene.hops), "6000", str(gs & 0xFFFFFFFF)],
+                         check=True, capture_output=True, text=True).stdout.split()
+    v = {out[i]: int(out[i + 1]) for i in range(0, len(out), 2)}
+    assert v["violations"] == 0 and v["tight_violations"] == 0
+    assert v["warps"] > 300 and v["tight_warps"] > 1000
+    assert v["culled"] > 0.3 * v["slots"]   # the warp test is doing work
+
