@@ -46,7 +46,7 @@ thread_local std::string g_last_error;
 // scan had measured 7 best (239.5 against 232 for 6). With the coherence sort and the warp
 // pre-cull, 6 -> 5 -> 4 blocks gave the single-view wavefront kernel 489.5 -> 493.0 -> 508.1
 // and the batched kernels (mix at spp / 16) 1170.8 -> 1210.2 -> 1172.2, so the two now have
-// caps of their own.
+// caps of their own; 3 blocks for the later hops measured 462.2, 6 for hop 0 508.6 (510.3).
 #ifndef HT_PERSIST_MINB
 #define HT_PERSIST_MINB 6
 #endif
