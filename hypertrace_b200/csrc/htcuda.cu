@@ -1880,6 +1880,7 @@ struct htc_batch {
     int num_sms, max_smem;
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
+    uint64_t *graph_stats;   // the stats buffer the graph's launches write
     std::vector<BatchView> h_views;
     // Two pinned staging slots for the asynchronous descriptor upload; slot i may be
     // rewritten once its last copy (event staged[i]) has run.
@@ -2049,6 +2050,9 @@ static int batch_grow(htc_batch *b, uint64_t slots, size_t words, uint32_t hops,
                                                                               hops <= b->sort_hops)))
         return HTC_OK;
     HTC_CUDA(cudaStreamSynchronize(st));
+    // a captured graph holds the old buffers' addresses: the next graph launch captures anew
+    if (b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     if (slots > b->wave_slots) {
         if (b->wave_buf) HTC_CUDA(cudaFree(b->wave_buf));
         b->wave_buf = nullptr;
@@ -2183,6 +2187,12 @@ int htc_batch_render(htc_batch *b, uint64_t *stats, void *stream) {
 int htc_batch_graph_launch(htc_batch *b, uint64_t *stats, void *stream) {
     if (!b) return fail(HTC_ERR_INVALID, "batch is NULL");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (b->graph_exec && b->graph_stats != stats) {   // the graph's kernels hold the stats pointer
+        cudaGraphExecDestroy(b->graph_exec);
+        b->graph_exec = nullptr;
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
     if (!b->graph_exec) {
         cudaStream_t cap;
         HTC_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
@@ -2198,6 +2208,7 @@ int htc_batch_graph_launch(htc_batch *b, uint64_t *stats, void *stream) {
         e = cudaGraphInstantiate(&b->graph_exec, g, 0);
         if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "cudaGraphInstantiate"); }
         b->graph = g;
+        b->graph_stats = stats;
     }
     HTC_CUDA(cudaGraphLaunch(b->graph_exec, st));
     return HTC_OK;

@@ -214,8 +214,9 @@ int htc_batch_reserve(htc_batch *batch, uint64_t pixels, uint32_t max_hops, void
 /* Renders every view's `passes`: one launch per pass index, hop depth and recipe over all the
  * views (wavefronts). stats as in htc_render_passes. */
 int htc_batch_render(htc_batch *batch, uint64_t *stats, void *stream);
-/* The same launch through a CUDA graph captured on first use (re-captured after
- * htc_batch_set_views); `stats` is baked into the graph at capture. */
+/* The same launch through a CUDA graph captured on first use and re-captured after
+ * htc_batch_set_views, after an htc_batch_reserve that grows the queues, and when `stats`
+ * differs from the pointer of the last capture (the graph's kernels hold it). */
 int htc_batch_graph_launch(htc_batch *batch, uint64_t *stats, void *stream);
 /* Reads and clears the batch's device error word (synchronises `stream`). */
 int htc_batch_check(htc_batch *batch, void *stream);

@@ -121,3 +121,36 @@ def test_batch_mixed_hop_counts(built):
     for a, b in zip(views, alone):
         assert torch.equal(a.canvas.seeds, b.canvas.seeds)
         assert torch.equal(a.canvas.image.view(torch.int32), b.canvas.image.view(torch.int32))
+
+
+def test_batch_graph_recaptures_for_new_stats_and_grown_queues(built):
+    """The captured graph's kernels hold the stats pointer and the queue buffers: a launch
+    with another stats buffer, and one after htc_batch_reserve grew the queues, capture anew —
+    the new buffer gets the statistics, the old one stays as it was, and the results still
+    equal the views rendered alone."""
+    ctx = P.Context(0)
+    views, alone = _views(5), _views(5)
+    for v in views + alone:
+        v.allocate(ctx)
+    br = B.BatchRenderer(ctx, max_views=16)
+    br.set_views(views, [2] * len(views), tile_pixels=256, blocks_per_sm=0)
+    s1 = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+    s2 = torch.zeros(8, dtype=torch.int64, device=ctx.device)
+    br.render(stats=s1, graph=True)
+    torch.cuda.synchronize()
+    first = s1.clone()
+    br.render(stats=s2, graph=True)
+    torch.cuda.synchronize()
+    assert torch.equal(s1, first)   # the second launch wrote to s2 only
+    n = 2 * sum(v.width * v.height for v in views)   # samples of two passes of every view
+    assert int(first[0]) == n and int(s2[0]) == n and int(s2[1]) > 0
+    br.reserve(4 * 1920 * 1080, 8)   # grows the queues (and the sort buffers) after a capture
+    br.render(stats=s2, graph=True)
+    br.check()
+    for v in alone:
+        P.Render(ctx, v.scene.recipe, v.scene.hops).render_passes(v.buffer, v.canvas, 6)
+    torch.cuda.synchronize()
+    assert int(s2[0]) == 2 * n and torch.equal(s1, first)
+    for a, b in zip(views, alone):
+        assert torch.equal(a.canvas.seeds, b.canvas.seeds)
+        assert torch.equal(a.canvas.image.view(torch.int32), b.canvas.image.view(torch.int32))
