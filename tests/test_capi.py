@@ -43,8 +43,19 @@ def test_errors_without_device(built):
     rc = _lib.lib().htc_program_create(3, 4, 32, 1, 0, ctypes.byref(h))   # double_support: HY / EU recipes only
     assert rc == _lib.HTC_ERR_UNSUPPORTED
     assert b"double_support" in _lib.lib().htc_last_error()
+    rc = _lib.lib().htc_program_create(1, 4, 32, 0, 4, ctypes.byref(h))   # no such flag bit
+    assert rc == _lib.HTC_ERR_INVALID
+    assert b"flags" in _lib.lib().htc_last_error()
     rc = _lib.lib().htc_render(None, 4, 4, None, 0, None, None, None)
     assert rc == _lib.HTC_ERR_INVALID
+
+
+def test_flag_values_match_header():
+    """The Python mirror's flag bits are the header's."""
+    text = open(os.path.join(ROOT, "include", "htcuda.h")).read()
+    flags = dict(re.findall(r"#define (HTC_FLAG_\w+) (\d+)u", text))
+    assert int(flags["HTC_FLAG_JITTER_YX"]) == _lib.HTC_FLAG_JITTER_YX
+    assert int(flags["HTC_FLAG_NO_SORT"]) == _lib.HTC_FLAG_NO_SORT
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
