@@ -217,7 +217,7 @@ __device__ bool stage_scene(const uint8_t *scene, size_t scene_size, uint32_t ma
         // the horospheres; ranks from a ballot per warp and the warps' counts in s_hdr[2..]
         const uint32_t h0 = (n_planes + 1) & ~1u;
         const uint32_t lane = tid & 31u, warp = tid >> 5, nwarps = (nthreads + 31) >> 5;
-        uint32_t before = 0;   // planes before this round
+        uint32_t before = 0;   // planes among the objects before this block-wide step
         for (uint32_t r0 = 0; r0 < n; r0 += nthreads) {
             const uint32_t k = r0 + tid;
             const bool in = k < n;
